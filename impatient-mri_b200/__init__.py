@@ -1,0 +1,249 @@
+"""Python binding of the IMPATIENT MRI B200 C-ABI (include/impatient_b200.h).
+
+The product is the sm_100a shared library ``libimpatient_b200.so`` and the
+``bin/mriSolver`` executable next to this file.  This module loads the library
+with ctypes and exposes the reference's operator and recon entry points under
+their reference names, on torch CUDA tensors (device pointers) or numpy
+arrays (host pointers).  There is no CPU fallback: if the library is missing
+or no GPU is visible, the calls raise.
+
+Names mirror the reference:
+    ftGpu / iftGpu                  kernels/ftGpu.cu:198, :653
+    parallelFtGpu / parallelIftGpu  kernels/parImagingGpu.cu:92, :119
+    bruteForceGpu                   bruteForce/bruteForceGpu.cuh:72-86
+    bruteForce                      main_mri.cuh:110-118 (directory level)
+    mriSolver                       main.cpp:103 (command line)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_PATH = PKG_DIR / "libimpatient_b200.so"
+MRISOLVER = PKG_DIR / "bin" / "mriSolver"
+
+IMP_OK = 0
+STATUS_NAMES = {
+    0: "IMP_OK", 1: "IMP_ERR_INVALID_ARG", 2: "IMP_ERR_CUDA", 3: "IMP_ERR_IO",
+    4: "IMP_ERR_FORMAT", 5: "IMP_ERR_RANGE", 6: "IMP_ERR_NOMEM", 7: "IMP_ERR_TIMEOUT",
+    8: "IMP_ERR_UNSUPPORTED",
+}
+
+# Every symbol include/impatient_b200.h declares (checked by the CPU tests).
+EXPORTED = [
+    "imp_abi_version", "imp_status_string", "imp_last_error",
+    "imp_context_create", "imp_context_destroy", "imp_context_synchronize",
+    "imp_context_launch_count", "imp_context_profile", "imp_context_profile_read",
+    "imp_ft", "imp_ift", "imp_parallel_ft", "imp_parallel_ift",
+    "imp_bf_options_default", "imp_bruteforce_recon", "imp_bruteforce_dir",
+    "imp_dataset_info", "imp_mrisolver_main", "imp_measure_alu_peaks",
+]
+
+
+class ImpError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class BfOptions(ctypes.Structure):
+    _fields_ = [
+        ("cg_num", ctypes.c_int), ("enable_fd", ctypes.c_int),
+        ("fd_penalizer", ctypes.c_float), ("enable_tv", ctypes.c_int),
+        ("tv_num", ctypes.c_int), ("tv_eps", ctypes.c_float), ("use_z", ctypes.c_int),
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Loads the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python impatient-mri_b200/build.py`")
+        L = ctypes.CDLL(str(LIB_PATH))
+        vp, ip, fp = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+        L.imp_last_error.restype = ctypes.c_char_p
+        L.imp_status_string.restype = ctypes.c_char_p
+        L.imp_status_string.argtypes = [ip]
+        L.imp_context_create.argtypes = [ip, ctypes.POINTER(vp)]
+        L.imp_context_destroy.argtypes = [vp]
+        L.imp_context_synchronize.argtypes = [vp]
+        L.imp_context_launch_count.argtypes = [vp]
+        L.imp_context_launch_count.restype = ctypes.c_long
+        L.imp_context_profile.argtypes = [vp, ip]
+        L.imp_context_profile_read.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double),
+                                               ctypes.POINTER(ctypes.c_long)]
+        op = [vp] + [vp] * 4 + [vp] * 8 + [ip, ip]
+        L.imp_ft.argtypes = op + [ip]
+        L.imp_ift.argtypes = op + [ip]
+        L.imp_parallel_ft.argtypes = op + [vp, vp, ip, ip]
+        L.imp_parallel_ift.argtypes = op + [vp, vp, ip, ip]
+        L.imp_bf_options_default.argtypes = [ctypes.POINTER(BfOptions)]
+        L.imp_bruteforce_recon.argtypes = ([vp, ctypes.POINTER(BfOptions)] + [vp] * 14
+                                           + [ip, ip, ip, ip])
+        L.imp_bruteforce_dir.argtypes = [ctypes.c_char_p, ctypes.c_char_p,
+                                         ctypes.POINTER(BfOptions), ip]
+        L.imp_dataset_info.argtypes = [ctypes.c_char_p] + [ctypes.POINTER(ctypes.c_int)] * 7
+        L.imp_mrisolver_main.argtypes = [ip, ctypes.POINTER(ctypes.c_char_p)]
+        L.imp_measure_alu_peaks.argtypes = [ip, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_double)]
+        _lib = L
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status != IMP_OK:
+        raise ImpError(status, lib().imp_last_error().decode())
+
+
+class Context:
+    """An imp_context: one CUDA stream and the device work memory."""
+
+    def __init__(self, device: int = 0):
+        self._h = ctypes.c_void_p()
+        _check(lib().imp_context_create(device, ctypes.byref(self._h)))
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def launch_count(self) -> int:
+        return int(lib().imp_context_launch_count(self._h))
+
+    def synchronize(self) -> None:
+        _check(lib().imp_context_synchronize(self._h))
+
+    def profile(self, enable: bool) -> None:
+        """Per-launch NUDFT kernel timing of recon calls (disables graphs)."""
+        _check(lib().imp_context_profile(self._h, int(enable)))
+
+    def profile_read(self):
+        """{'forward': (total_ms, launches), 'adjoint': (total_ms, launches)}"""
+        out = {}
+        for i, name in enumerate(("forward", "adjoint")):
+            ms, n = ctypes.c_double(), ctypes.c_long()
+            _check(lib().imp_context_profile_read(self._h, i, ctypes.byref(ms), ctypes.byref(n)))
+            out[name] = (ms.value, n.value)
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            lib().imp_context_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _ptr(a):
+    """Device (torch CUDA tensor) or host (numpy / CPU tensor) float32 pointer."""
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        if a.dtype.__str__() != "torch.float32" or not a.is_contiguous():
+            raise TypeError("tensors must be contiguous float32")
+        return ctypes.c_void_p(a.data_ptr())
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.float32 or not a.flags.c_contiguous:
+            raise TypeError("arrays must be C-contiguous float32")
+        return ctypes.c_void_p(a.ctypes.data)
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def ftGpu(ctx, kdata_r, kdata_i, idata_r, idata_i, kx, ky, kz, ix, iy, iz, fm, t,
+          num_k, num_i, use_z=0):
+    _check(lib().imp_ft(ctx.handle, *map(_ptr, (kdata_r, kdata_i, idata_r, idata_i, kx, ky, kz,
+                                                ix, iy, iz, fm, t)), num_k, num_i, use_z))
+
+
+def iftGpu(ctx, idata_r, idata_i, kdata_r, kdata_i, kx, ky, kz, ix, iy, iz, fm, t,
+           num_k, num_i, use_z=0):
+    _check(lib().imp_ift(ctx.handle, *map(_ptr, (idata_r, idata_i, kdata_r, kdata_i, kx, ky, kz,
+                                                 ix, iy, iz, fm, t)), num_k, num_i, use_z))
+
+
+def parallelFtGpu(ctx, kdata_r, kdata_i, idata_r, idata_i, kx, ky, kz, ix, iy, iz, fm, t,
+                  num_k, num_i, sensi_r, sensi_i, num_coil, use_z=0):
+    _check(lib().imp_parallel_ft(ctx.handle, *map(_ptr, (kdata_r, kdata_i, idata_r, idata_i,
+                                                         kx, ky, kz, ix, iy, iz, fm, t)),
+                                 num_k, num_i, _ptr(sensi_r), _ptr(sensi_i), num_coil, use_z))
+
+
+def parallelIftGpu(ctx, idata_r, idata_i, kdata_r, kdata_i, kx, ky, kz, ix, iy, iz, fm, t,
+                   num_k, num_i, sensi_r, sensi_i, num_coil, use_z=0):
+    _check(lib().imp_parallel_ift(ctx.handle, *map(_ptr, (idata_r, idata_i, kdata_r, kdata_i,
+                                                          kx, ky, kz, ix, iy, iz, fm, t)),
+                                  num_k, num_i, _ptr(sensi_r), _ptr(sensi_i), num_coil, use_z))
+
+
+def bf_options(cg_num=8, fd_penalizer=None, tv=False, tv_num=10, tv_eps=1e-6, use_z=0,
+               dims=None) -> BfOptions:
+    """Options of the brute-force recon; fd_penalizer enables the FD term
+    (as -fdp does, main.cpp:306-316).  dims = (nx, ny, nz) sets the TV grid."""
+    o = BfOptions()
+    lib().imp_bf_options_default(ctypes.byref(o))
+    o.cg_num = cg_num
+    o.enable_fd = 1 if fd_penalizer is not None else 0
+    o.fd_penalizer = float(fd_penalizer or 0.0)
+    o.enable_tv = 1 if tv else 0
+    o.tv_num = tv_num
+    o.tv_eps = float(tv_eps)
+    o.use_z = int(use_z)
+    if dims is not None:
+        o.nx, o.ny, o.nz = (int(d) for d in dims)
+    return o
+
+
+def bruteForceGpu(ctx, opts: BfOptions, idata_r, idata_i, kdata_r, kdata_i, kx, ky, kz, ix, iy,
+                  iz, fm, t, sensi_r, sensi_i, num_k, num_i, num_coil, num_slices=1):
+    """In-place brute-force CG: idata_* hold the initial estimate and receive the image."""
+    _check(lib().imp_bruteforce_recon(
+        ctx.handle, ctypes.byref(opts), *map(_ptr, (idata_r, idata_i, kdata_r, kdata_i, kx, ky,
+                                                    kz, ix, iy, iz, fm, t, sensi_r, sensi_i)),
+        num_k, num_i, num_coil, num_slices))
+
+
+def bruteForce(idir: str, odir: str, opts: BfOptions, gpu_id: int = 0) -> None:
+    _check(lib().imp_bruteforce_dir(os.fsencode(idir), os.fsencode(odir), ctypes.byref(opts),
+                                    gpu_id))
+
+
+def dataset_info(idir: str) -> dict:
+    """Sizes of an input directory as the reference reader sees them (no GPU)."""
+    v = [ctypes.c_int(0) for _ in range(7)]
+    _check(lib().imp_dataset_info(os.fsencode(idir), *(ctypes.byref(x) for x in v)))
+    keys = ("num_k", "num_i", "num_coil", "num_slices", "nx", "ny", "nz")
+    return {k: x.value for k, x in zip(keys, v)}
+
+
+def measure_alu_peaks(device: int = 0):
+    """(FP32 FMA TFLOP/s, SFU sine G ops/s) measured on `device`."""
+    f, s = ctypes.c_double(), ctypes.c_double()
+    _check(lib().imp_measure_alu_peaks(device, ctypes.byref(f), ctypes.byref(s)))
+    return f.value, s.value
+
+
+def mriSolver(*args: str) -> int:
+    """Runs the mriSolver command line in-process; returns its exit code."""
+    argv = [b"mriSolver"] + [os.fsencode(a) for a in args]
+    arr = (ctypes.c_char_p * (len(argv) + 1))(*argv, None)
+    return int(lib().imp_mrisolver_main(len(argv), arr))

@@ -1,0 +1,85 @@
+// Internal host-side interface of the NUDFT tile engine.
+//
+// The engine evaluates, for every (sample k, voxel r) pair,
+//     theta = 2 pi (kx x + ky y + kz z) + omega_r t_k
+// (the exponent of kernels/ftCpu.cpp:158-160, with the z term of
+// toeplitz/computeFH.cmem.cu:185-188 when use_z is set) and
+//     F   : y_c[k] += S_c[r] x[r] e^{-i theta}        (kernels/ftGpu.cu:306-604)
+//     F^H : x[r]   += conj(S_c[r]) d_c[k] e^{+i theta} (kernels/ftGpu.cu:756-1013)
+//
+// Phase arithmetic: the four products are accumulated in FP64 on top of the
+// constant 1.5*2^20 turns, so that the low 32 bits of the double's mantissa
+// are the phase modulo one turn in units of 2^-32 turn (an exact fixed-point
+// reduction; no FP32 rounding of large arguments).  The top 23 of those bits
+// become an FP32 angle in [-pi, pi) for the hardware sin/cos.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace imp {
+
+constexpr int kNT = 128;     // threads per NUDFT block
+constexpr int kTile = 64;    // "theirs" elements per shared-memory tile
+constexpr int kPadM = 1024;  // sample / voxel counts are padded to this
+
+struct NuLaunch {
+    int pt = 4;     // "ours" elements per thread
+    int split = 1;  // partitions of the "theirs" range (partial sums)
+};
+
+struct NuPlan {
+    int M = 0, N = 0, C = 0;     // samples, voxels, coils
+    int CG = 1, G = 1;           // coils per group, groups (CG * G >= C)
+    int Mpad = 0, Npad = 0;
+    bool use_z = false;
+    double4 *kgeo = nullptr;     // [Mpad]  (kx, ky, kz, t)        turns / s
+    double4 *vgeo = nullptr;     // [Npad]  (x, y, z, omega/2pi)   FOV / Hz
+    float2 *sens = nullptr;      // [G][Npad][CG] coil sensitivities (zero padded)
+    NuLaunch fwd, adj;
+};
+
+// Creates geometry and packed sensitivities from device SoA inputs.
+// sensi_r/sensi_i may be null (unit sensitivity, C must be 1).
+cudaError_t nu_plan_create(NuPlan &p, const float *kx, const float *ky, const float *kz,
+                           const float *t, const float *ix, const float *iy, const float *iz,
+                           const float *fm, const float *sensi_r, const float *sensi_i, int M,
+                           int N, int C, bool use_z, unsigned *dev_err, cudaStream_t st);
+// Replaces only the field map (per-slice) of an existing plan.
+cudaError_t nu_plan_set_fm(NuPlan &p, const float *fm, unsigned *dev_err, cudaStream_t st);
+void nu_plan_destroy(NuPlan &p);
+
+// Heuristic launch shape (replaced by the autotuner when enabled).
+NuLaunch nu_default_launch(const NuPlan &p, bool adj);
+
+// Scratch bytes for the partial sums of one apply.
+size_t nu_fwd_partial_bytes(const NuPlan &p, const NuLaunch &l);
+size_t nu_adj_partial_bytes(const NuPlan &p, const NuLaunch &l);
+
+// xs[g][r][cg] = S[g][r][cg] * x[r]   (x interleaved complex, [Npad])
+cudaError_t nu_pack_image(const NuPlan &p, const float2 *x, float2 *xs, cudaStream_t st);
+// Same from SoA x (operator API).
+cudaError_t nu_pack_image_soa(const NuPlan &p, const float *xr, const float *xi, float2 *xs,
+                              cudaStream_t st);
+
+// Forward partials: part[split][g][Mpad][CG].
+cudaError_t nu_forward_partials(const NuPlan &p, const NuLaunch &l, const float2 *xs,
+                                float2 *part, unsigned *dev_err, cudaStream_t st);
+// Adjoint partials (after conj(S) and the in-group coil sum): part[split][g][Npad].
+// `data` is [G][Mpad][CG].
+cudaError_t nu_adjoint_partials(const NuPlan &p, const NuLaunch &l, const float2 *data,
+                                float2 *part, unsigned *dev_err, cudaStream_t st);
+
+// k-space SoA [C][M] <-> packed [G][Mpad][CG]
+cudaError_t nu_pack_kdata(const NuPlan &p, const float *dr, const float *di, float2 *packed,
+                          cudaStream_t st);
+// Sum forward partials and write SoA [C][M] (operator API).
+cudaError_t nu_forward_finish_soa(const NuPlan &p, const NuLaunch &l, const float2 *part,
+                                  float *yr, float *yi, cudaStream_t st);
+// Sum adjoint partials and write SoA [N].
+cudaError_t nu_adjoint_finish_soa(const NuPlan &p, const NuLaunch &l, const float2 *part,
+                                  float *xr, float *xi, cudaStream_t st);
+
+// Kernel selection exposed for the autotuner: time one launch shape.
+bool nu_shape_supported(int CG, int pt);
+
+}  // namespace imp

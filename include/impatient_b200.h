@@ -1,0 +1,160 @@
+/*
+ * impatient_b200.h -- C-ABI of the B200 (sm_100a) rebuild of the IMPATIENT MRI
+ * iterative non-Cartesian reconstruction path (mriSolver).
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Complex vectors are split real/imag
+ *     float32 arrays (the reference's SoA layout).  Coil-indexed arrays are
+ *     coil-major: sensi[c*num_i + r], kdata[c*num_k + k].
+ *   - Every entry point returns an imp_status (0 = IMP_OK) and never exits the
+ *     process; imp_last_error() gives a message for the calling thread.
+ *   - An imp_context owns one CUDA stream and the device work memory; use one
+ *     context per thread.  Operator-level calls take DEVICE pointers and are
+ *     synchronous.  Recon-level calls accept host or device pointers.
+ *   - The reference's interfaces that each entry point replaces are cited as
+ *     path:line within the reference project.
+ */
+#ifndef IMPATIENT_B200_H
+#define IMPATIENT_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int imp_status;
+
+#define IMP_OK 0
+#define IMP_ERR_INVALID_ARG 1  /* bad size, null pointer, inconsistent flags      */
+#define IMP_ERR_CUDA 2         /* a CUDA runtime call failed                       */
+#define IMP_ERR_IO 3           /* file missing / unreadable / unwritable           */
+#define IMP_ERR_FORMAT 4       /* malformed 0.2 / 1.0 input file                   */
+#define IMP_ERR_RANGE 5        /* coordinate outside the fixed-point phase range   */
+#define IMP_ERR_NOMEM 6        /* device allocation failed                         */
+#define IMP_ERR_TIMEOUT 7      /* a bounded device-side wait expired               */
+#define IMP_ERR_UNSUPPORTED 8  /* option the library does not implement            */
+
+/* Version of this ABI (major*100 + minor). */
+int imp_abi_version(void);
+const char *imp_status_string(imp_status s);
+/* Message of the last failing call on this thread ("" if none). */
+const char *imp_last_error(void);
+
+typedef struct imp_context imp_context;
+
+/* Creates a context on CUDA device `device` with its own stream (a blocking
+ * stream: it orders after work queued on the legacy default stream). */
+imp_status imp_context_create(int device, imp_context **ctx);
+imp_status imp_context_destroy(imp_context *ctx);
+/* Blocks until all work of the context's stream is done. */
+imp_status imp_context_synchronize(imp_context *ctx);
+/* Number of this library's kernels launched by the most recent call. */
+long imp_context_launch_count(const imp_context *ctx);
+
+/* Kernel timing of recon calls (no reference counterpart; replaces the
+ * reference's cutil timer singleton, kernels/structures.h:206-601).  While
+ * enabled, recon calls run without CUDA graphs and bracket every NUDFT launch
+ * with CUDA events on the launching stream; enabling resets the totals. */
+imp_status imp_context_profile(imp_context *ctx, int enable);
+/* which: 0 = forward NUDFT kernel, 1 = adjoint NUDFT kernel. */
+imp_status imp_context_profile_read(const imp_context *ctx, int which, double *total_ms,
+                                    long *count);
+
+/* Measures the FP32 FMA rate (TFLOP/s, 2 flops per FMA) and the SFU sine rate
+ * (G ops/s) of `device` with two short throughput kernels: the denominators
+ * of the NUDFT roofline.  No reference counterpart. */
+imp_status imp_measure_alu_peaks(int device, double *fp32_tflops, double *sfu_gops);
+
+/* ------------------------------------------------------------------------
+ * Operator level: NUDFT with field map (DEVICE pointers, synchronous).
+ * theta(k,r) = 2 pi (kx[k] ix[r] + ky[k] iy[r] + use_z*kz[k] iz[r]) + fm[r] t[k]
+ * use_z = 0 reproduces the reference, whose NUDFT drops z
+ * (kernels/ftGpu.cu:325-328); use_z = 1 is the 3-D formula of
+ * toeplitz/computeFH.cmem.cu:185-188.  fm may be NULL (no field map).
+ * ---------------------------------------------------------------------- */
+
+/* kdata[k] = sum_r idata[r] exp(-i theta)
+ * replaces ftGpu(), kernels/ftGpu.cu:198 / kernels/gpuPrototypes.cuh:154 */
+imp_status imp_ft(imp_context *ctx, float *kdata_r, float *kdata_i, const float *idata_r,
+                  const float *idata_i, const float *kx, const float *ky, const float *kz,
+                  const float *ix, const float *iy, const float *iz, const float *fm,
+                  const float *t, int num_k, int num_i, int use_z);
+
+/* idata[r] = sum_k kdata[k] exp(+i theta)
+ * replaces iftGpu(), kernels/ftGpu.cu:653 / kernels/gpuPrototypes.cuh:162 */
+imp_status imp_ift(imp_context *ctx, float *idata_r, float *idata_i, const float *kdata_r,
+                   const float *kdata_i, const float *kx, const float *ky, const float *kz,
+                   const float *ix, const float *iy, const float *iz, const float *fm,
+                   const float *t, int num_k, int num_i, int use_z);
+
+/* kdata[c*num_k + k] = sum_r sensi[c*num_i + r] idata[r] exp(-i theta)
+ * replaces parallelFtGpu(), kernels/parImagingGpu.cu:92 */
+imp_status imp_parallel_ft(imp_context *ctx, float *kdata_r, float *kdata_i,
+                           const float *idata_r, const float *idata_i, const float *kx,
+                           const float *ky, const float *kz, const float *ix, const float *iy,
+                           const float *iz, const float *fm, const float *t, int num_k,
+                           int num_i, const float *sensi_r, const float *sensi_i, int num_coil,
+                           int use_z);
+
+/* idata[r] = sum_c conj(sensi[c*num_i + r]) sum_k kdata[c*num_k + k] exp(+i theta)
+ * replaces parallelIftGpu(), kernels/parImagingGpu.cu:119 */
+imp_status imp_parallel_ift(imp_context *ctx, float *idata_r, float *idata_i,
+                            const float *kdata_r, const float *kdata_i, const float *kx,
+                            const float *ky, const float *kz, const float *ix, const float *iy,
+                            const float *iz, const float *fm, const float *t, int num_k,
+                            int num_i, const float *sensi_r, const float *sensi_i,
+                            int num_coil, int use_z);
+
+/* ------------------------------------------------------------------------
+ * Recon level: brute-force CG (host or device pointers).
+ * ---------------------------------------------------------------------- */
+typedef struct imp_bf_options {
+    int cg_num;          /* CG iteration number; cg_num-1 updates are made  */
+    int enable_fd;       /* finite-difference regularizer (-fd / -fdp)      */
+    float fd_penalizer;  /* lambda (-fdp)                                   */
+    int enable_tv;       /* TV reweighting outer loop (-tv)                 */
+    int tv_num;          /* TV iterations (-tv_num)                         */
+    float tv_eps;        /* TV smoothing, reference FP32 value 1e-6         */
+    int use_z;           /* 0: reference 2-D semantics, 1: true 3-D         */
+    int nx, ny, nz;      /* TV grid.  0,0,0 = reference sqrt(N) x sqrt(N)   */
+} imp_bf_options;
+
+/* Fills `opt` with the reference defaults (main.cpp:96-101). */
+void imp_bf_options_default(imp_bf_options *opt);
+
+/* Brute-force CG recon of one or more slices.  idata (num_slices*num_i) is the
+ * initial estimate on entry and the image on return; kdata is
+ * [slice][coil][num_k]; fm is [slice][num_i]; trajectories, t and sensi are
+ * shared by all slices, as in the reference's slice loop.
+ * replaces bruteForceGpu(), bruteForce/bruteForceGpu.cuh:72-86 (called per
+ * slice from bruteForce(), main_mri.cu:875-895) */
+imp_status imp_bruteforce_recon(imp_context *ctx, const imp_bf_options *opt, float *idata_r,
+                                float *idata_i, const float *kdata_r, const float *kdata_i,
+                                const float *kx, const float *ky, const float *kz,
+                                const float *ix, const float *iy, const float *iz,
+                                const float *fm, const float *t, const float *sensi_r,
+                                const float *sensi_i, int num_k, int num_i, int num_coil,
+                                int num_slices);
+
+/* Directory-level drop-in of bruteForce(idir, odir, ...) (main_mri.cuh:110-118,
+ * main_mri.cu:652-1025): reads idir in the 0.2 or 1.0 format
+ * (kernels/structures.cpp:569-1162), reconstructs every slice and writes
+ * odir/output_gpu_r.dat and odir/output_gpu_i.dat as "%f\n" text
+ * (kernels/structures.cpp:1165-1175). */
+imp_status imp_bruteforce_dir(const char *idir, const char *odir, const imp_bf_options *opt,
+                              int gpu_id);
+
+/* Reads the sizes of an input directory with the reference's reader rules
+ * (loadInputData, kernels/structures.cpp:569-780) without touching a GPU.
+ * Any output pointer may be NULL. */
+imp_status imp_dataset_info(const char *idir, int *num_k, int *num_i, int *num_coil,
+                            int *num_slices, int *nx, int *ny, int *nz);
+
+/* The mriSolver command line (main.cpp:103-444) as a library call: same
+ * flags, defaults and exit codes (0 ok, 1 error). */
+int imp_mrisolver_main(int argc, char **argv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMPATIENT_B200_H */

@@ -1,0 +1,117 @@
+"""Brute-force CG on the GPU against the reference's FP64 recon (golden
+vectors) and the FP64 oracle.  Tolerance: 1e-4 relative L2 on the final
+image after the same iteration count and semantics (cg_num-1 updates)."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+TOL_IMG = 1e-4
+
+
+@pytest.fixture(scope="module")
+def ctx(pkg):
+    c = pkg.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module", autouse=True)
+def built():
+    oracle.build(ref=False)
+
+
+def test_bf_2d_tv_matches_reference_fp64(pkg, ctx):
+    from gpu_util import gpu_recon
+    c = golden("bf_2d")
+    x = gpu_recon(pkg, ctx, c, cg_num=int(c["cg_num"]), lam=float(c["lam"]), tv=True,
+                  tv_num=int(c["tv_num"]), eps=1e-7)
+    err = oracle.rel_l2(x, c["x64"])
+    err32 = oracle.rel_l2(c["x32"], c["x64"])
+    print(f"GPU vs reference FP64: {err:.2e}; reference FP32 vs FP64: {err32:.2e}")
+    assert err < TOL_IMG
+
+
+def test_bf_2d_sense_matches_reference_fp64(pkg, ctx):
+    from gpu_util import gpu_recon
+    c = golden("bf_2d_c3")
+    x = gpu_recon(pkg, ctx, c, cg_num=int(c["cg_num"]), lam=float(c["lam"]), tv=False, eps=1e-7)
+    assert oracle.rel_l2(x, c["x64"]) < TOL_IMG
+
+
+def small_3d(synth, seed=31):
+    rng = np.random.default_rng(seed)
+    ny = nx = 24
+    nz = 8
+    kx2, ky2, t2 = synth.spiral(4, 128, 12.0, rng)
+    kz = np.repeat(np.arange(-4, 4, dtype=np.float32), kx2.size)
+    case = dict(kx=np.tile(kx2, 8), ky=np.tile(ky2, 8), kz=kz, t=np.tile(t2, 8))
+    ix, iy, iz = synth.grid_positions(ny, nx, nz)
+    img = synth.ellipse_phantom((ny, nx, nz), 5, rng)
+    case.update(ix=ix, iy=iy, iz=iz, fm=synth.field_map((ny, nx, nz), rng).ravel(),
+                sens=synth.coil_maps((ny, nx, nz), 4, rng).reshape(4, -1), dims=(nx, ny, nz),
+                opts=dict(use_z=1, cg_num=6))
+    y = oracle.ft(img.ravel(), case, use_z=1)
+    case["kdata"] = synth.add_noise(y, 40.0, rng).astype(np.complex64)
+    return case
+
+
+def test_bf_3d_tv_matches_oracle(pkg, ctx, synth):
+    from gpu_util import gpu_recon
+    c = small_3d(synth)
+    x = gpu_recon(pkg, ctx, c, cg_num=6, lam=1e-3, tv=True, tv_num=2, eps=1e-6, use_z=1,
+                  dims=c["dims"])
+    ref = oracle.bf_cg(c, cg_num=6, lam=1e-3, tv=True, tv_num=2, eps=1e-6, use_z=1)
+    assert oracle.rel_l2(x, ref) < TOL_IMG
+
+
+def test_host_and_device_pointers_agree(pkg, ctx):
+    from gpu_util import gpu_recon
+    c = golden("bf_2d_c3")
+    a = gpu_recon(pkg, ctx, c, cg_num=4, lam=1e-2, tv=False, host_ptrs=True)
+    b = gpu_recon(pkg, ctx, c, cg_num=4, lam=1e-2, tv=False, host_ptrs=False)
+    assert np.array_equal(a, b)
+
+
+def test_multi_slice_equals_slice_by_slice(pkg, ctx):
+    from gpu_util import gpu_recon
+    c = golden("bf_2d_c3")
+    rng = np.random.default_rng(2)
+    kd2 = c["kdata"] * (0.5 + 0.1j) + 0.01 * rng.standard_normal(c["kdata"].shape)
+    fm2 = (c["fm"] * -0.7).astype(np.float32)
+    both = dict(c, kdata=np.concatenate([c["kdata"].ravel(), kd2.ravel()]),
+                fm=np.concatenate([c["fm"], fm2]))
+    x = gpu_recon(pkg, ctx, both, cg_num=5, lam=1e-2, tv=True, tv_num=2)
+    a = gpu_recon(pkg, ctx, c, cg_num=5, lam=1e-2, tv=True, tv_num=2)
+    b = gpu_recon(pkg, ctx, dict(c, kdata=kd2, fm=fm2), cg_num=5, lam=1e-2, tv=True, tv_num=2)
+    N = c["ix"].size
+    assert np.array_equal(x[:N], a) and np.array_equal(x[N:], b)
+
+
+def test_warm_start_from_idata(pkg, ctx):
+    """idata is the initial estimate (bruteForceCpu starts from *idata)."""
+    from gpu_util import gpu_recon
+    c = golden("bf_2d_c3")
+    x0 = oracle.bf_cg(c, cg_num=3, lam=1e-2, tv=False, eps=1e-6, use_z=0).astype(np.complex64)
+    x = gpu_recon(pkg, ctx, c, x0=x0, cg_num=4, lam=1e-2, tv=False)
+    ref = oracle.bf_cg(c, x0=x0, cg_num=4, lam=1e-2, tv=False, eps=1e-6, use_z=0)
+    assert oracle.rel_l2(x, ref) < TOL_IMG
+
+
+def test_cli_end_to_end(pkg, tmp_path):
+    """mriSolver on a 0.2-format directory writes output_gpu_{r,i}.dat ("%f")."""
+    from impatient_mri_b200 import io
+    c = golden("bf_2d")
+    io.write_dataset(tmp_path / "in", "0.2", kx=c["kx"], ky=c["ky"], kz=c["kz"], t=c["t"],
+                     ix=c["ix"], iy=c["iy"], iz=c["iz"], fm=c["fm"], kdata=c["kdata"],
+                     sensi=c["sens"], dims=(64, 64, 1))
+    rc = pkg.mriSolver("-idir", str(tmp_path / "in"), "-odir", str(tmp_path / "out"),
+                       "-cg_num", "6", "-fdp", "0.001", "-tv_num", "3")
+    assert rc == 0
+    xr = np.loadtxt(tmp_path / "out" / "output_gpu_r.dat")
+    xi = np.loadtxt(tmp_path / "out" / "output_gpu_i.dat")
+    ref = oracle.bf_cg(c, cg_num=6, lam=1e-3, tv=True, tv_num=3, eps=1e-6, use_z=0)
+    # "%f" keeps 6 decimals
+    assert np.max(np.abs(xr + 1j * xi - ref)) < 1e-5 + 1e-4 * np.max(np.abs(ref))
