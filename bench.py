@@ -345,8 +345,38 @@ def run_ours(args, ws, rank, local):
     return 0
 
 
+def run_nudft_only(args, local):
+    """Forward + adjoint NUDFT applies of the benchmark geometry through the
+    operator C-ABI (the small command the kernel profiles are taken on)."""
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from impatient_mri_b200 import synth
+    torch.cuda.set_device(local)
+    case = synth.make_case(WORKLOAD)
+    M, N, C = case["M"], case["N"], case["num_coil"]
+    f = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32)).cuda()
+    g = {k: f(case[k]) for k in ("kx", "ky", "kz", "t", "ix", "iy", "iz", "fm")}
+    sr, si = f(case["sens"].real), f(case["sens"].imag)
+    xr, xi = f(case["x_true"].real), f(case["x_true"].imag)
+    yr = torch.zeros(C * M, device="cuda")
+    yi = torch.zeros(C * M, device="cuda")
+    with pkg.Context(local) as ctx:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            pkg.parallelFtGpu(ctx, yr, yi, xr, xi, g["kx"], g["ky"], g["kz"], g["ix"], g["iy"],
+                              g["iz"], g["fm"], g["t"], M, N, sr, si, C, 1)
+            pkg.parallelIftGpu(ctx, xr, xi, yr, yi, g["kx"], g["ky"], g["kz"], g["ix"],
+                               g["iy"], g["iz"], g["fm"], g["t"], M, N, sr, si, C, 1)
+        dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    print(json.dumps({"nudft_only": WORKLOAD, "ms_per_fwd_adj_pair": dt * 1e3}))
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
+    ap.add_argument("--nudft-only", action="store_true",
+                    help="only forward + adjoint NUDFT applies (profiling command)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -355,6 +385,8 @@ def main() -> int:
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     try:
+        if args.nudft_only:
+            return run_nudft_only(args, local)
         if args.impl == "reference":
             return run_reference(args, ws, rank)
         return run_ours(args, ws, rank, local)
