@@ -115,6 +115,7 @@ imp_status run_forward(imp_context *ctx, float *yr, float *yi, const float *xr, 
     IMP_CUDA(imp::nu_plan_create(g.p, kx, ky, kz, t, ix, iy, iz, fm, sr, si, M, N, C,
                                  use_z != 0, ctx->dev_err, ctx->stream),
              "plan");
+    imp::nu_tuned_lookup(g.p, false, &g.p.fwd);
     const size_t xs_b = align256(sizeof(float2) * (size_t)g.p.G * g.p.Npad * g.p.CG);
     const size_t pf_b = align256(imp::nu_fwd_partial_bytes(g.p, g.p.fwd));
     void *w = nullptr;
@@ -141,6 +142,7 @@ imp_status run_adjoint(imp_context *ctx, float *xr, float *xi, const float *dr, 
     IMP_CUDA(imp::nu_plan_create(g.p, kx, ky, kz, t, ix, iy, iz, fm, sr, si, M, N, C,
                                  use_z != 0, ctx->dev_err, ctx->stream),
              "plan");
+    imp::nu_tuned_lookup(g.p, true, &g.p.adj);
     const size_t dp_b = align256(sizeof(float2) * (size_t)g.p.G * g.p.Mpad * g.p.CG);
     const size_t pa_b = align256(imp::nu_adj_partial_bytes(g.p, g.p.adj));
     void *w = nullptr;

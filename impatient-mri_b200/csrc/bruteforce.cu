@@ -332,8 +332,21 @@ cudaError_t BfSolver::setup(const BfConfig &cfg, const float *kx, const float *k
     IMP_TRY(dalloc(&g_, plan_.Npad));
     IMP_TRY(dalloc(&d_, plan_.Npad));
     IMP_TRY(dalloc(&w_, plan_.Npad));
-    IMP_TRY(cudaMalloc(&pf_, nu_fwd_partial_bytes(plan_, plan_.fwd)));
-    IMP_TRY(cudaMalloc(&pa_, nu_adj_partial_bytes(plan_, plan_.adj)));
+    // partial-sum scratch sized for every shape the autotuner may pick
+    size_t pf_bytes = nu_fwd_partial_bytes(plan_, plan_.fwd);
+    size_t pa_bytes = nu_adj_partial_bytes(plan_, plan_.adj);
+    if (cfg.autotune) {
+        pf_bytes = std::max(pf_bytes, nu_tune_partial_bytes(plan_, false));
+        pa_bytes = std::max(pa_bytes, nu_tune_partial_bytes(plan_, true));
+    }
+    IMP_TRY(cudaMalloc(&pf_, pf_bytes));
+    IMP_TRY(cudaMalloc(&pa_, pa_bytes));
+    if (cfg.autotune) {
+        IMP_TRY(cudaMemsetAsync(xs_, 0, sizeof(float2) * nxs, st_));
+        IMP_TRY(cudaMemsetAsync(rpk_, 0, sizeof(float2) * nk, st_));
+        IMP_TRY(nu_autotune(plan_, false, xs_, pf_, pf_bytes, err_, st_, &plan_.fwd));
+        IMP_TRY(nu_autotune(plan_, true, rpk_, pa_, pa_bytes, err_, st_, &plan_.adj));
+    }
     IMP_TRY(dalloc(&dots_, (size_t)5 * kDotBlocks));
     IMP_TRY(cudaMemsetAsync(dots_, 0, sizeof(double) * 5 * kDotBlocks, st_));
     return cudaGetLastError();

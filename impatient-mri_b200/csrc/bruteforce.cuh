@@ -17,6 +17,7 @@ struct BfConfig {
     int tv_num = 1;
     float tv_eps = 1e-6f;        // MRI_SMOOTH_FACTOR (FP32 build)
     bool use_graphs = true;
+    bool autotune = true;        // time launch shapes once per problem shape
 };
 
 class BfSolver {

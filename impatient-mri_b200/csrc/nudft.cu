@@ -30,8 +30,8 @@ constexpr double kMagic = 1572864.0 + 0.5 + 5.9604644775390625e-08;
 constexpr float kTwoPiF = 6.28318530717958647692f;
 constexpr float kThreePiF = 9.42477796076937971538f;
 
-template <int CG, int PT, bool USEZ, bool ADJ>
-__global__ void __launch_bounds__(kNT, 4)
+template <int CG, int PT, bool USEZ, bool ADJ, int OCC>
+__global__ void __launch_bounds__(kNT, OCC)
     k_nudft(const double4 *__restrict__ ours, const double4 *__restrict__ theirs,
             const float2 *__restrict__ tdata, const float2 *__restrict__ sens,
             float2 *__restrict__ out, int n_ours_pad, int n_theirs_pad, int per_split,
@@ -300,19 +300,20 @@ inline int grid_for(size_t n, int bs = 256) {
 
 // ------------------------------ dispatch -----------------------------------
 
-template <int CG, int PT, bool ADJ>
+template <int CG, int PT, bool ADJ, int OCC>
 cudaError_t launch_cg_pt(const NuPlan &p, int split, const double4 *ours, const double4 *theirs,
                          const float2 *tdata, float2 *out, unsigned *err, cudaStream_t st) {
     const int n_ours = ADJ ? p.Npad : p.Mpad;
     const int n_theirs = ADJ ? p.Mpad : p.Npad;
+    if (!nu_split_ok(n_theirs, split)) return cudaErrorInvalidConfiguration;
     const int per_split = n_theirs / split;
     dim3 grid(n_ours / (kNT * PT), split, p.G);
     if (p.use_z)
-        k_nudft<CG, PT, true, ADJ><<<grid, kNT, 0, st>>>(ours, theirs, tdata, p.sens, out, n_ours,
-                                                         n_theirs, per_split, err);
+        k_nudft<CG, PT, true, ADJ, OCC><<<grid, kNT, 0, st>>>(ours, theirs, tdata, p.sens, out,
+                                                              n_ours, n_theirs, per_split, err);
     else
-        k_nudft<CG, PT, false, ADJ><<<grid, kNT, 0, st>>>(ours, theirs, tdata, p.sens, out,
-                                                          n_ours, n_theirs, per_split, err);
+        k_nudft<CG, PT, false, ADJ, OCC><<<grid, kNT, 0, st>>>(ours, theirs, tdata, p.sens, out,
+                                                               n_ours, n_theirs, per_split, err);
     return cudaGetLastError();
 }
 
@@ -321,9 +322,13 @@ cudaError_t launch_nudft(const NuPlan &p, const NuLaunch &l, const float2 *tdata
                          unsigned *err, cudaStream_t st) {
     const double4 *ours = ADJ ? p.vgeo : p.kgeo;
     const double4 *theirs = ADJ ? p.kgeo : p.vgeo;
-#define IMP_CASE(CGV, PTV)                                                                \
-    if (p.CG == CGV && l.pt == PTV)                                                       \
-        return launch_cg_pt<CGV, PTV, ADJ>(p, l.split, ours, theirs, tdata, out, err, st);
+#define IMP_CASE(CGV, PTV)                                                                   \
+    if (p.CG == CGV && l.pt == PTV) {                                                        \
+        if (l.occ == 6)                                                                      \
+            return launch_cg_pt<CGV, PTV, ADJ, 6>(p, l.split, ours, theirs, tdata, out, err, \
+                                                  st);                                       \
+        return launch_cg_pt<CGV, PTV, ADJ, 4>(p, l.split, ours, theirs, tdata, out, err, st); \
+    }
     IMP_CASE(1, 4)
     IMP_CASE(1, 8)
     IMP_CASE(2, 4)
@@ -335,6 +340,11 @@ cudaError_t launch_nudft(const NuPlan &p, const NuLaunch &l, const float2 *tdata
 }
 
 }  // namespace
+
+bool nu_split_ok(int n_theirs, int split) {
+    return split >= 1 && n_theirs % split == 0 && (n_theirs / split) % kTile == 0 &&
+           n_theirs / split >= kTile;
+}
 
 bool nu_shape_supported(int CG, int pt) {
     return (CG == 1 && (pt == 4 || pt == 8)) || (CG == 2 && pt == 4) ||
@@ -358,7 +368,7 @@ NuLaunch nu_default_launch(const NuPlan &p, bool adj) {
     const long blocks = (long)(n_ours / (kNT * l.pt)) * p.G;
     const long target = 148L * 4 * 2;  // two waves at four blocks per SM
     int split = 1;
-    while (blocks * split < target && split < 64 && (n_theirs / (split * 2)) % kTile == 0 &&
+    while (blocks * split < target && split < 64 && nu_split_ok(n_theirs, split * 2) &&
            n_theirs / (split * 2) >= 4 * kTile)
         split *= 2;
     l.split = split;

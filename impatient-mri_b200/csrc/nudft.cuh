@@ -25,6 +25,7 @@ constexpr int kPadM = 1024;  // sample / voxel counts are padded to this
 struct NuLaunch {
     int pt = 4;     // "ours" elements per thread
     int split = 1;  // partitions of the "theirs" range (partial sums)
+    int occ = 4;    // blocks per SM the register budget is sized for (4 or 6)
 };
 
 struct NuPlan {
@@ -79,7 +80,20 @@ cudaError_t nu_forward_finish_soa(const NuPlan &p, const NuLaunch &l, const floa
 cudaError_t nu_adjoint_finish_soa(const NuPlan &p, const NuLaunch &l, const float2 *part,
                                   float *xr, float *xi, cudaStream_t st);
 
-// Kernel selection exposed for the autotuner: time one launch shape.
+// Launch shapes the kernel set covers.
 bool nu_shape_supported(int CG, int pt);
+// True when `split` partitions n_theirs into whole shared-memory tiles.
+bool nu_split_ok(int n_theirs, int split);
+
+// Autotuner (tune.cu): times every supported (pt, occ, split) of one direction
+// on the live buffers `tdata` / `part` (part_bytes of scratch) and returns the
+// fastest.  Results are cached per problem shape in memory and in a text file
+// ($IMP_TUNE_CACHE, default ~/.cache/impatient_b200/nudft_tune.txt).
+cudaError_t nu_autotune(const NuPlan &p, bool adj, const float2 *tdata, float2 *part,
+                        size_t part_bytes, unsigned *dev_err, cudaStream_t st, NuLaunch *out);
+// Cached result for this shape, if any (no timing).
+bool nu_tuned_lookup(const NuPlan &p, bool adj, NuLaunch *out);
+// Largest partial-sum scratch any tuning candidate needs.
+size_t nu_tune_partial_bytes(const NuPlan &p, bool adj);
 
 }  // namespace imp

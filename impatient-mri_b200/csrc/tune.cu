@@ -1,0 +1,176 @@
+// Project autotuner for the NUDFT tile engine.
+//
+// For one problem shape and direction it times every launch shape the kernel
+// set covers -- "ours" elements per thread (pt), register budget (occupancy
+// 4 or 6 blocks per SM) and the number of partitions of the "theirs" range
+// (split) -- with CUDA events on the launching stream, and keeps the fastest.
+// Results are cached per shape in memory and persisted as text lines
+//     v1 <adj> <CG> <G> <use_z> <Mpad> <Npad> <pt> <occ> <split> <ms>
+// in $IMP_TUNE_CACHE (default ~/.cache/impatient_b200/nudft_tune.txt), so a
+// shape is tuned once per machine.  IMP_AUTOTUNE=0 turns tuning off.
+#include "nudft.cuh"
+
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+#include <sys/stat.h>
+#include <tuple>
+#include <vector>
+
+namespace imp {
+
+namespace {
+
+using Key = std::tuple<int, int, int, int, int, int>;
+
+std::mutex g_mu;
+std::map<Key, NuLaunch> g_cache;
+bool g_loaded = false;
+
+Key key_of(const NuPlan &p, bool adj) {
+    return Key(adj ? 1 : 0, p.CG, p.G, p.use_z ? 1 : 0, p.Mpad, p.Npad);
+}
+
+std::string cache_path() {
+    if (const char *e = std::getenv("IMP_TUNE_CACHE")) return e;
+    const char *h = std::getenv("HOME");
+    return std::string(h ? h : "/tmp") + "/.cache/impatient_b200/nudft_tune.txt";
+}
+
+void load_locked() {
+    if (g_loaded) return;
+    g_loaded = true;
+    FILE *f = std::fopen(cache_path().c_str(), "r");
+    if (!f) return;
+    char tag[8];
+    int a, cg, g, z, mp, np, pt, occ, split;
+    double ms;
+    while (std::fscanf(f, "%7s %d %d %d %d %d %d %d %d %d %lf", tag, &a, &cg, &g, &z, &mp, &np,
+                       &pt, &occ, &split, &ms) == 11) {
+        if (std::string(tag) != "v1") continue;
+        NuLaunch l;
+        l.pt = pt;
+        l.occ = occ;
+        l.split = split;
+        if (nu_shape_supported(cg, pt) && (occ == 4 || occ == 6))
+            g_cache[Key(a, cg, g, z, mp, np)] = l;
+    }
+    std::fclose(f);
+}
+
+void persist(const Key &k, const NuLaunch &l, double ms) {
+    std::string path = cache_path();
+    // create the parent directories
+    for (size_t i = 1; i < path.size(); ++i)
+        if (path[i] == '/') mkdir(path.substr(0, i).c_str(), 0755);
+    FILE *f = std::fopen(path.c_str(), "a");
+    if (!f) return;  // the cache is an optimisation; failure to write is not an error
+    std::fprintf(f, "v1 %d %d %d %d %d %d %d %d %d %.4f\n", std::get<0>(k), std::get<1>(k),
+                 std::get<2>(k), std::get<3>(k), std::get<4>(k), std::get<5>(k), l.pt, l.occ,
+                 l.split, ms);
+    std::fclose(f);
+}
+
+bool tuning_enabled() {
+    const char *e = std::getenv("IMP_AUTOTUNE");
+    return !(e && e[0] == '0');
+}
+
+std::vector<int> pts_for(int CG) {
+    std::vector<int> v;
+    for (int pt : {2, 4, 8})
+        if (nu_shape_supported(CG, pt)) v.push_back(pt);
+    return v;
+}
+
+constexpr int kMaxSplit = 64;
+constexpr size_t kMaxPartialBytes = size_t(512) << 20;
+
+}  // namespace
+
+size_t nu_tune_partial_bytes(const NuPlan &p, bool adj) {
+    const int n_theirs = adj ? p.Mpad : p.Npad;
+    size_t best = 0;
+    for (int s = 1; s <= kMaxSplit; s *= 2) {
+        if (!nu_split_ok(n_theirs, s)) continue;
+        NuLaunch l;
+        l.split = s;
+        const size_t b = adj ? nu_adj_partial_bytes(p, l) : nu_fwd_partial_bytes(p, l);
+        if (b <= kMaxPartialBytes && b > best) best = b;
+    }
+    return best;
+}
+
+bool nu_tuned_lookup(const NuPlan &p, bool adj, NuLaunch *out) {
+    std::lock_guard<std::mutex> g(g_mu);
+    load_locked();
+    auto it = g_cache.find(key_of(p, adj));
+    if (it == g_cache.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+cudaError_t nu_autotune(const NuPlan &p, bool adj, const float2 *tdata, float2 *part,
+                        size_t part_bytes, unsigned *dev_err, cudaStream_t st, NuLaunch *out) {
+    *out = nu_default_launch(p, adj);
+    if (nu_tuned_lookup(p, adj, out)) {
+        const size_t need = adj ? nu_adj_partial_bytes(p, *out) : nu_fwd_partial_bytes(p, *out);
+        if (need <= part_bytes) return cudaSuccess;
+        *out = nu_default_launch(p, adj);
+    }
+    if (!tuning_enabled()) return cudaSuccess;
+    const int n_theirs = adj ? p.Mpad : p.Npad;
+    cudaEvent_t e0, e1;
+    cudaError_t e;
+    if ((e = cudaEventCreate(&e0)) != cudaSuccess) return e;
+    if ((e = cudaEventCreate(&e1)) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return e;
+    }
+    float best = 1e30f;
+    NuLaunch best_l = *out;
+    for (int pt : pts_for(p.CG))
+        for (int occ : {4, 6})
+            for (int s = 1; s <= kMaxSplit; s *= 2) {
+                if (!nu_split_ok(n_theirs, s)) continue;
+                NuLaunch l;
+                l.pt = pt;
+                l.occ = occ;
+                l.split = s;
+                const size_t need = adj ? nu_adj_partial_bytes(p, l) : nu_fwd_partial_bytes(p, l);
+                if (need > part_bytes) continue;
+                auto run = [&]() {
+                    return adj ? nu_adjoint_partials(p, l, tdata, part, dev_err, st)
+                               : nu_forward_partials(p, l, tdata, part, dev_err, st);
+                };
+                if ((e = run()) != cudaSuccess) break;  // warm-up
+                float ms_min = 1e30f;
+                for (int rep = 0; rep < 2; ++rep) {
+                    cudaEventRecord(e0, st);
+                    if ((e = run()) != cudaSuccess) break;
+                    cudaEventRecord(e1, st);
+                    cudaEventSynchronize(e1);
+                    float ms = 0.f;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    ms_min = ms < ms_min ? ms : ms_min;
+                }
+                if (e != cudaSuccess) break;
+                if (ms_min < best) {
+                    best = ms_min;
+                    best_l = l;
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return e;
+    *out = best_l;
+    std::lock_guard<std::mutex> g(g_mu);
+    load_locked();
+    g_cache[key_of(p, adj)] = best_l;
+    persist(key_of(p, adj), best_l, best);
+    return cudaSuccess;
+}
+
+}  // namespace imp
