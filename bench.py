@@ -179,7 +179,7 @@ def run_reference(args, ws, rank):
         print(json.dumps({"impl": "reference",
                           "unavailable": "reference CPU build oracle/_ref missing"}))
         return 0
-    sample_k = 256
+    sample_k = 2048
     cores = os.cpu_count()
     vals = []
     for i in range(args.warmup + args.steps):
@@ -330,10 +330,10 @@ def run_ours(args, ws, rank, local):
         try:
             import oracle
             if oracle.ref_available("bf32_omp"):
-                v, dt = cpu_reference_sample(case, 256)
+                v, dt = cpu_reference_sample(case, 8192)
                 out["cpu_baseline"] = {
                     "value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                    "sample": (f"reference parallelFtCpu (FP32, OpenMP) on 256 of {M} samples x "
+                    "sample": (f"reference parallelFtCpu (FP32, OpenMP) on 8192 of {M} samples x "
                                f"{N} voxels x {C} coils ({dt:.1f} s), extrapolated to "
                                f"{applies_per_recon()} applies per recon")}
         except Exception as e:  # the baseline is reported, never required

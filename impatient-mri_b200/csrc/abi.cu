@@ -22,6 +22,7 @@ struct imp_context {
     bool prof_on = false;         // per-launch NUDFT timing (imp_context_profile)
     double prof_ms[2] = {0.0, 0.0};
     long prof_count[2] = {0, 0};
+    std::unique_ptr<imp::BfSolver> bf;  // brute-force solver reused across calls
 };
 
 namespace {
@@ -226,6 +227,7 @@ imp_status imp_context_destroy(imp_context *ctx) {
     if (!ctx) return IMP_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->bf.reset();
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->dev_err) cudaFree(ctx->dev_err);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -359,7 +361,10 @@ imp_status imp_bruteforce_recon(imp_context *ctx, const imp_bf_options *opt, flo
         d_sr = nullptr;  // one coil: unit sensitivity (kernels/structures.cpp:710-716)
         d_si = nullptr;
     }
-    imp::BfSolver solver;
+    // the context keeps one solver: buffers, tuned shapes and CUDA graphs are
+    // reused by later calls of the same problem size
+    if (!ctx->bf) ctx->bf.reset(new imp::BfSolver());
+    imp::BfSolver &solver = *ctx->bf;
     IMP_CUDA(solver.setup(cfg, d_kx, d_ky, d_kz, d_t, d_ix, d_iy, d_iz, d_sr, d_si, ctx->dev_err,
                           ctx->stream),
              "brute-force setup");

@@ -314,6 +314,20 @@ cudaError_t BfSolver::setup(const BfConfig &cfg, const float *kx, const float *k
                             const float *kz, const float *t, const float *ix, const float *iy,
                             const float *iz, const float *sensi_r, const float *sensi_i,
                             unsigned *dev_err, cudaStream_t st) {
+    const bool same_shape = plan_.kgeo && st == st_ && dev_err == err_ && cfg.M == cfg_.M &&
+                            cfg.N == cfg_.N && cfg.C == cfg_.C && cfg.use_z == cfg_.use_z &&
+                            cfg.n0 == cfg_.n0 && cfg.n1 == cfg_.n1 && cfg.n2 == cfg_.n2 &&
+                            cfg.autotune == cfg_.autotune;
+    if (same_shape) {
+        // keep buffers, tuned launch shapes and (if the captured scalars match) the graphs
+        if (cfg.fd != cfg_.fd || cfg.lambda != cfg_.lambda) {
+            if (g_iter_) cudaGraphExecDestroy(g_iter_);
+            if (g_init_) cudaGraphExecDestroy(g_init_);
+            g_iter_ = g_init_ = nullptr;
+        }
+        cfg_ = cfg;
+        return nu_plan_repack(plan_, kx, ky, kz, t, ix, iy, iz, sensi_r, sensi_i, dev_err, st);
+    }
     release();
     cfg_ = cfg;
     st_ = st;

@@ -375,6 +375,19 @@ NuLaunch nu_default_launch(const NuPlan &p, bool adj) {
     return l;
 }
 
+static cudaError_t pack_geometry(NuPlan &p, const float *kx, const float *ky, const float *kz,
+                                 const float *t, const float *ix, const float *iy,
+                                 const float *iz, const float *fm, const float *sensi_r,
+                                 const float *sensi_i, unsigned *dev_err, cudaStream_t st) {
+    k_pack_kgeo<<<(p.Mpad + 255) / 256, 256, 0, st>>>(p.kgeo, kx, ky, kz, t, p.M, p.Mpad,
+                                                       p.use_z ? 1 : 0, dev_err);
+    k_pack_vgeo<<<(p.Npad + 255) / 256, 256, 0, st>>>(p.vgeo, ix, iy, iz, fm, p.N, p.Npad,
+                                                       p.use_z ? 1 : 0, dev_err);
+    k_pack_sens<<<grid_for((size_t)p.G * p.Npad * p.CG), 256, 0, st>>>(
+        p.sens, sensi_r, sensi_i, p.N, p.Npad, p.C, p.CG, p.G);
+    return cudaGetLastError();
+}
+
 cudaError_t nu_plan_create(NuPlan &p, const float *kx, const float *ky, const float *kz,
                            const float *t, const float *ix, const float *iy, const float *iz,
                            const float *fm, const float *sensi_r, const float *sensi_i, int M,
@@ -393,15 +406,16 @@ cudaError_t nu_plan_create(NuPlan &p, const float *kx, const float *ky, const fl
     if ((e = cudaMalloc(&p.vgeo, sizeof(double4) * p.Npad)) != cudaSuccess) return e;
     if ((e = cudaMalloc(&p.sens, sizeof(float2) * (size_t)p.G * p.Npad * p.CG)) != cudaSuccess)
         return e;
-    k_pack_kgeo<<<(p.Mpad + 255) / 256, 256, 0, st>>>(p.kgeo, kx, ky, kz, t, M, p.Mpad,
-                                                       use_z ? 1 : 0, dev_err);
-    k_pack_vgeo<<<(p.Npad + 255) / 256, 256, 0, st>>>(p.vgeo, ix, iy, iz, fm, N, p.Npad,
-                                                       use_z ? 1 : 0, dev_err);
-    k_pack_sens<<<grid_for((size_t)p.G * p.Npad * p.CG), 256, 0, st>>>(
-        p.sens, sensi_r, sensi_i, N, p.Npad, C, p.CG, p.G);
     p.fwd = nu_default_launch(p, false);
     p.adj = nu_default_launch(p, true);
-    return cudaGetLastError();
+    return pack_geometry(p, kx, ky, kz, t, ix, iy, iz, fm, sensi_r, sensi_i, dev_err, st);
+}
+
+cudaError_t nu_plan_repack(NuPlan &p, const float *kx, const float *ky, const float *kz,
+                           const float *t, const float *ix, const float *iy, const float *iz,
+                           const float *sensi_r, const float *sensi_i, unsigned *dev_err,
+                           cudaStream_t st) {
+    return pack_geometry(p, kx, ky, kz, t, ix, iy, iz, nullptr, sensi_r, sensi_i, dev_err, st);
 }
 
 cudaError_t nu_plan_set_fm(NuPlan &p, const float *fm, unsigned *dev_err, cudaStream_t st) {

@@ -45,6 +45,11 @@ cudaError_t nu_plan_create(NuPlan &p, const float *kx, const float *ky, const fl
                            const float *t, const float *ix, const float *iy, const float *iz,
                            const float *fm, const float *sensi_r, const float *sensi_i, int M,
                            int N, int C, bool use_z, unsigned *dev_err, cudaStream_t st);
+// Re-packs geometry and sensitivities of the same sizes into an existing plan.
+cudaError_t nu_plan_repack(NuPlan &p, const float *kx, const float *ky, const float *kz,
+                           const float *t, const float *ix, const float *iy, const float *iz,
+                           const float *sensi_r, const float *sensi_i, unsigned *dev_err,
+                           cudaStream_t st);
 // Replaces only the field map (per-slice) of an existing plan.
 cudaError_t nu_plan_set_fm(NuPlan &p, const float *fm, unsigned *dev_err, cudaStream_t st);
 void nu_plan_destroy(NuPlan &p);

@@ -90,6 +90,21 @@ def test_host_and_device_pointers_agree(pkg, ctx):
     assert np.array_equal(a, b)
 
 
+def test_context_reuse_matches_fresh_context(pkg, ctx, synth):
+    """A context keeps its solver between calls of the same size; a second
+    geometry of that size must give what a fresh context gives."""
+    from gpu_util import gpu_recon
+    c = golden("bf_2d")
+    rng = np.random.default_rng(9)
+    kx, ky, t = synth.spiral(4, 1024, 32.0, rng)
+    c2 = dict(c, kx=kx, ky=ky, t=t, fm=(c["fm"] * 0.3).astype(np.float32))
+    gpu_recon(pkg, ctx, c, cg_num=3, lam=1e-2, tv=True, tv_num=2)
+    a = gpu_recon(pkg, ctx, c2, cg_num=3, lam=1e-2, tv=True, tv_num=2)
+    with pkg.Context(0) as fresh:
+        b = gpu_recon(pkg, fresh, c2, cg_num=3, lam=1e-2, tv=True, tv_num=2)
+    assert np.array_equal(a, b)
+
+
 def test_multi_slice_equals_slice_by_slice(pkg, ctx):
     from gpu_util import gpu_recon
     c = golden("bf_2d_c3")
