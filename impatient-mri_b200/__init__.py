@@ -38,7 +38,7 @@ EXPORTED = [
     "imp_abi_version", "imp_status_string", "imp_last_error",
     "imp_context_create", "imp_context_destroy", "imp_context_synchronize",
     "imp_context_launch_count", "imp_context_profile", "imp_context_profile_read",
-    "imp_ft", "imp_ift", "imp_parallel_ft", "imp_parallel_ift",
+    "imp_ft", "imp_ift", "imp_parallel_ft", "imp_parallel_ift", "imp_parallel_ift_noalloc",
     "imp_bf_options_default", "imp_bruteforce_recon", "imp_bruteforce_dir",
     "imp_dataset_info", "imp_mrisolver_main", "imp_measure_alu_peaks",
 ]
@@ -87,6 +87,7 @@ def lib() -> ctypes.CDLL:
         L.imp_ift.argtypes = op + [ip]
         L.imp_parallel_ft.argtypes = op + [vp, vp, ip, ip]
         L.imp_parallel_ift.argtypes = op + [vp, vp, ip, ip]
+        L.imp_parallel_ift_noalloc.argtypes = [vp] * 12 + [ip, ip, vp, vp, ip, ip, vp]
         L.imp_bf_options_default.argtypes = [ctypes.POINTER(BfOptions)]
         L.imp_bruteforce_recon.argtypes = ([vp, ctypes.POINTER(BfOptions)] + [vp] * 14
                                            + [ip, ip, ip, ip])

@@ -423,6 +423,30 @@ cudaError_t nu_plan_set_fm(NuPlan &p, const float *fm, unsigned *dev_err, cudaSt
     return cudaGetLastError();
 }
 
+void nu_plan_dims(NuPlan &p, int M, int N, int C, bool use_z) {
+    p.M = M;
+    p.N = N;
+    p.C = C;
+    p.CG = choose_cg(C);
+    p.G = (C + p.CG - 1) / p.CG;
+    p.Mpad = round_up(std::max(M, 1), kPadM);
+    p.Npad = round_up(std::max(N, 1), kPadM);
+    p.use_z = use_z;
+}
+
+cudaError_t nu_plan_place(NuPlan &p, double4 *kgeo, double4 *vgeo, float2 *sens,
+                          const float *kx, const float *ky, const float *kz, const float *t,
+                          const float *ix, const float *iy, const float *iz, const float *fm,
+                          const float *sensi_r, const float *sensi_i, unsigned *dev_err,
+                          cudaStream_t st) {
+    p.kgeo = kgeo;
+    p.vgeo = vgeo;
+    p.sens = sens;
+    p.fwd = nu_default_launch(p, false);
+    p.adj = nu_default_launch(p, true);
+    return pack_geometry(p, kx, ky, kz, t, ix, iy, iz, fm, sensi_r, sensi_i, dev_err, st);
+}
+
 void nu_plan_destroy(NuPlan &p) {
     if (p.kgeo) cudaFree(p.kgeo);
     if (p.vgeo) cudaFree(p.vgeo);

@@ -50,6 +50,16 @@ cudaError_t nu_plan_repack(NuPlan &p, const float *kx, const float *ky, const fl
                            const float *t, const float *ix, const float *iy, const float *iz,
                            const float *sensi_r, const float *sensi_i, unsigned *dev_err,
                            cudaStream_t st);
+// Sizes of a plan (M, N, C, CG, G, Mpad, Npad, use_z) without any memory.
+void nu_plan_dims(NuPlan &p, int M, int N, int C, bool use_z);
+// Packs geometry into caller-provided device memory (kgeo [Mpad], vgeo
+// [Npad], sens [G][Npad][CG]) of a plan sized by nu_plan_dims.  Nothing is
+// allocated; such a plan must not be passed to nu_plan_destroy.
+cudaError_t nu_plan_place(NuPlan &p, double4 *kgeo, double4 *vgeo, float2 *sens,
+                          const float *kx, const float *ky, const float *kz, const float *t,
+                          const float *ix, const float *iy, const float *iz, const float *fm,
+                          const float *sensi_r, const float *sensi_i, unsigned *dev_err,
+                          cudaStream_t st);
 // Replaces only the field map (per-slice) of an existing plan.
 cudaError_t nu_plan_set_fm(NuPlan &p, const float *fm, unsigned *dev_err, cudaStream_t st);
 void nu_plan_destroy(NuPlan &p);

@@ -104,6 +104,30 @@ imp_status imp_parallel_ift(imp_context *ctx, float *idata_r, float *idata_i,
                             int num_i, const float *sensi_r, const float *sensi_i,
                             int num_coil, int use_z);
 
+/* The same adjoint as imp_parallel_ift, for callers that cannot allocate
+ * device memory -- for example a reconstruction host that reserves all device
+ * memory through its own allocator at start-up or runs under a fixed memory
+ * budget.  No counterpart in the reference.
+ *   - Allocates nothing and needs no context: all work memory (packed
+ *     geometry, sensitivities and k-space data, partial sums) is one static
+ *     device array of 32 MiB that every GPU loading this library holds until
+ *     the process exits.  Sizes whose work memory does not fit are rejected
+ *     with IMP_ERR_INVALID_ARG.  About 40 bytes per voxel and 40 bytes per
+ *     sample per group of up to 8 coils are needed, plus partial sums.
+ *   - Runs on `stream` (a cudaStream_t; NULL is the legacy default stream) of
+ *     the current device and returns when the result is in idata.
+ *   - The first call on a device looks up the device address of the array
+ *     with that device current; make that first call before any stream
+ *     capture.
+ *   - Every call shares the array: calls that overlap on the GPU race. */
+imp_status imp_parallel_ift_noalloc(float *idata_r, float *idata_i, const float *kdata_r,
+                                    const float *kdata_i, const float *kx, const float *ky,
+                                    const float *kz, const float *ix, const float *iy,
+                                    const float *iz, const float *fm, const float *t,
+                                    int num_k, int num_i, const float *sensi_r,
+                                    const float *sensi_i, int num_coil, int use_z,
+                                    void *stream);
+
 /* ------------------------------------------------------------------------
  * Recon level: brute-force CG (host or device pointers).
  * ---------------------------------------------------------------------- */
