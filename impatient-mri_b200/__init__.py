@@ -41,6 +41,8 @@ EXPORTED = [
     "imp_ft", "imp_ift", "imp_parallel_ft", "imp_parallel_ift", "imp_parallel_ift_noalloc",
     "imp_bf_options_default", "imp_bruteforce_recon", "imp_bruteforce_dir",
     "imp_dataset_info", "imp_mrisolver_main", "imp_measure_alu_peaks",
+    "imp_toeplitz_options_default", "imp_toeplitz_q", "imp_toeplitz_fhd", "imp_toeplitz_recon",
+    "imp_toeplitz_apply", "imp_toeplitz_dir",
 ]
 
 
@@ -56,6 +58,15 @@ class BfOptions(ctypes.Structure):
         ("fd_penalizer", ctypes.c_float), ("enable_tv", ctypes.c_int),
         ("tv_num", ctypes.c_int), ("tv_eps", ctypes.c_float), ("use_z", ctypes.c_int),
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+    ]
+
+
+class ToepOptions(ctypes.Structure):
+    _fields_ = [
+        ("cg_num", ctypes.c_int), ("enable_fd", ctypes.c_int),
+        ("fd_penalizer", ctypes.c_float), ("enable_tv", ctypes.c_int),
+        ("tv_num", ctypes.c_int), ("tv_eps", ctypes.c_float), ("ntime_segs", ctypes.c_float),
+        ("gridOS_Q", ctypes.c_float), ("gridOS_FH", ctypes.c_float),
     ]
 
 
@@ -97,6 +108,13 @@ def lib() -> ctypes.CDLL:
         L.imp_mrisolver_main.argtypes = [ip, ctypes.POINTER(ctypes.c_char_p)]
         L.imp_measure_alu_peaks.argtypes = [ip, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double)]
+        TO = ctypes.POINTER(ToepOptions)
+        L.imp_toeplitz_options_default.argtypes = [TO]
+        L.imp_toeplitz_q.argtypes = [vp, TO] + [vp] * 6 + [ip] * 4
+        L.imp_toeplitz_fhd.argtypes = [vp, TO] + [vp] * 11 + [ip] * 5
+        L.imp_toeplitz_recon.argtypes = [vp, TO] + [vp] * 7 + [ip] + [vp] * 3 + [ip] * 4
+        L.imp_toeplitz_apply.argtypes = [vp, TO] + [vp] * 7 + [ip] + [vp] * 3 + [ip] * 4
+        L.imp_toeplitz_dir.argtypes = [ctypes.c_char_p, TO, ip, ip, ip, ctypes.c_char_p, ip]
         _lib = L
     return _lib
 
@@ -241,6 +259,60 @@ def measure_alu_peaks(device: int = 0):
     f, s = ctypes.c_double(), ctypes.c_double()
     _check(lib().imp_measure_alu_peaks(device, ctypes.byref(f), ctypes.byref(s)))
     return f.value, s.value
+
+
+def toeplitz_options(cg_num=8, fd_penalizer=None, tv=False, tv_num=10, tv_eps=1e-6,
+                     ntime_segs=12.0, gridOS_Q=1.125, gridOS_FH=1.5) -> ToepOptions:
+    """Options of the Toeplitz recon; fd_penalizer enables the FD term."""
+    o = ToepOptions()
+    lib().imp_toeplitz_options_default(ctypes.byref(o))
+    o.cg_num = cg_num
+    o.enable_fd = 1 if fd_penalizer is not None else 0
+    o.fd_penalizer = float(fd_penalizer or 0.0)
+    o.enable_tv = 1 if tv else 0
+    o.tv_num = tv_num
+    o.tv_eps = float(tv_eps)
+    o.ntime_segs = float(ntime_segs)
+    o.gridOS_Q = float(gridOS_Q)
+    o.gridOS_FH = float(gridOS_FH)
+    return o
+
+
+def toeplitz_q(ctx, opts: ToepOptions, q_r, q_i, kx, ky, kz, t, num_k, nx, ny, nz=1):
+    """Q_l for l = 0..L into q_r/q_i ((L+1) x 2N-grid floats each)."""
+    _check(lib().imp_toeplitz_q(ctx.handle, ctypes.byref(opts),
+                                *map(_ptr, (q_r, q_i, kx, ky, kz, t)), num_k, nx, ny, nz))
+
+
+def toeplitz_fhd(ctx, opts: ToepOptions, fhd_r, fhd_i, kdata_r, kdata_i, kx, ky, kz, t, fm,
+                 sensi_r, sensi_i, num_k, num_coil, nx, ny, nz=1):
+    _check(lib().imp_toeplitz_fhd(
+        ctx.handle, ctypes.byref(opts), *map(_ptr, (fhd_r, fhd_i, kdata_r, kdata_i, kx, ky, kz,
+                                                    t, fm, sensi_r, sensi_i)),
+        num_k, num_coil, nx, ny, nz))
+
+
+def toeplitz_recon(ctx, opts: ToepOptions, x_r, x_i, fhd_r, fhd_i, q_r, q_i, t, num_k, fm,
+                   sensi_r, sensi_i, num_coil, nx, ny, nz=1):
+    _check(lib().imp_toeplitz_recon(
+        ctx.handle, ctypes.byref(opts), *map(_ptr, (x_r, x_i, fhd_r, fhd_i, q_r, q_i, t)),
+        num_k, _ptr(fm), _ptr(sensi_r), _ptr(sensi_i), num_coil, nx, ny, nz))
+
+
+def toeplitz_apply(ctx, opts: ToepOptions, out_r, out_i, p_r, p_i, q_r, q_i, t, num_k, fm,
+                   sensi_r, sensi_i, num_coil, nx, ny, nz=1):
+    _check(lib().imp_toeplitz_apply(
+        ctx.handle, ctypes.byref(opts), *map(_ptr, (out_r, out_i, p_r, p_i, q_r, q_i, t)),
+        num_k, _ptr(fm), _ptr(sensi_r), _ptr(sensi_i), num_coil, nx, ny, nz))
+
+
+def toeplitz(idir: str, opts: ToepOptions, direct=False, gpu_id=0, reuseQ=False, Qdir=None,
+             writeQ=False) -> None:
+    """Directory-level Toeplitz recon: writes idir/FhD.file, idir/out.file
+    (and idir/Q_stone.file with writeQ)."""
+    _check(lib().imp_toeplitz_dir(os.fsencode(idir), ctypes.byref(opts), int(direct), gpu_id,
+                                  int(reuseQ), os.fsencode(Qdir) if Qdir else None,
+                                  int(writeQ)))
 
 
 def mriSolver(*args: str) -> int:

@@ -2,8 +2,10 @@
 #include "../../include/impatient_b200.h"
 #include "bruteforce.cuh"
 #include "common.cuh"
+#include "context.h"
 #include "io.h"
 #include "nudft.cuh"
+#include "toeplitz.cuh"
 
 #include <cmath>
 #include <cstdio>
@@ -12,22 +14,13 @@
 #include <string>
 #include <vector>
 
-struct imp_context {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    unsigned *dev_err = nullptr;  // device error word (imp::DEV_ERR_*)
-    long launches = 0;
-    void *scratch = nullptr;      // grow-only work memory of the operator calls
-    size_t scratch_bytes = 0;
-    bool prof_on = false;         // per-launch NUDFT timing (imp_context_profile)
-    double prof_ms[2] = {0.0, 0.0};
-    long prof_count[2] = {0, 0};
-    std::unique_ptr<imp::BfSolver> bf;  // brute-force solver reused across calls
-};
+imp_context::~imp_context() = default;
+
+namespace imp {
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
 imp_status fail(imp_status s, const std::string &msg) {
     g_last_error = msg;
@@ -39,12 +32,6 @@ imp_status from_cuda(cudaError_t e, const char *what) {
     const imp_status s = e == cudaErrorMemoryAllocation ? IMP_ERR_NOMEM : IMP_ERR_CUDA;
     return fail(s, std::string(what) + ": " + cudaGetErrorString(e));
 }
-
-#define IMP_CUDA(call, what)                                      \
-    do {                                                          \
-        imp_status s_ = from_cuda((call), what);                  \
-        if (s_ != IMP_OK) return s_;                              \
-    } while (0)
 
 // Makes `ctx` current and clears its device error word.
 imp_status begin(imp_context *ctx) {
@@ -70,6 +57,15 @@ imp_status finish(imp_context *ctx) {
         return fail(IMP_ERR_TIMEOUT, "a bounded device-side wait expired");
     return IMP_OK;
 }
+
+}  // namespace imp
+
+using imp::begin;
+using imp::fail;
+using imp::finish;
+using imp::from_cuda;
+
+namespace {
 
 imp_status scratch(imp_context *ctx, size_t bytes, void **p) {
     if (bytes > ctx->scratch_bytes) {
@@ -158,19 +154,25 @@ imp_status run_adjoint(imp_context *ctx, float *xr, float *xi, const float *dr, 
 }
 
 // Host or device pointer -> device pointer (copies host data into `keep`).
-imp_status to_device(imp_context *ctx, const float *p, size_t n,
-                     std::vector<std::unique_ptr<void, void (*)(void *)>> &keep,
+}  // namespace
+
+namespace imp {
+
+static bool is_device_ptr(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+imp_status to_device(imp_context *ctx, const float *p, size_t n, DevKeep &keep,
                      const float **out, bool *was_host) {
     *out = p;
     if (was_host) *was_host = false;
     if (!p || n == 0) return IMP_OK;
-    cudaPointerAttributes a;
-    cudaError_t e = cudaPointerGetAttributes(&a, p);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        a.type = cudaMemoryTypeUnregistered;
-    }
-    if (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) return IMP_OK;
+    if (is_device_ptr(p)) return IMP_OK;
     void *d = nullptr;
     IMP_CUDA(cudaMalloc(&d, n * sizeof(float)), "input staging");
     keep.emplace_back(d, [](void *q) { cudaFree(q); });
@@ -181,7 +183,24 @@ imp_status to_device(imp_context *ctx, const float *p, size_t n,
     return IMP_OK;
 }
 
-}  // namespace
+imp_status out_device(imp_context *ctx, float *p, size_t n, DevKeep &keep, float **out,
+                      bool *was_host) {
+    (void)ctx;
+    *out = p;
+    *was_host = false;
+    if (!p || n == 0) return IMP_OK;
+    if (is_device_ptr(p)) return IMP_OK;
+    void *d = nullptr;
+    IMP_CUDA(cudaMalloc(&d, n * sizeof(float)), "output staging");
+    keep.emplace_back(d, [](void *q) { cudaFree(q); });
+    *out = (float *)d;
+    *was_host = true;
+    return IMP_OK;
+}
+
+}  // namespace imp
+
+using imp::to_device;
 
 extern "C" {
 
@@ -202,7 +221,7 @@ const char *imp_status_string(imp_status s) {
     }
 }
 
-const char *imp_last_error(void) { return g_last_error.c_str(); }
+const char *imp_last_error(void) { return imp::g_last_error.c_str(); }
 
 imp_status imp_context_create(int device, imp_context **out) {
     if (!out) return fail(IMP_ERR_INVALID_ARG, "null output pointer");
@@ -228,6 +247,7 @@ imp_status imp_context_destroy(imp_context *ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->bf.reset();
+    ctx->tp.reset();
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->dev_err) cudaFree(ctx->dev_err);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

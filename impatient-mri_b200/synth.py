@@ -123,8 +123,10 @@ def make_case(name: str, seed: int | None = None, forward=None, small: bool = Fa
 
     names: "bf2d_64"        64x64, 1 coil, 4 x 1024 spiral, 8 CG, TV 1e-3
            "bf3d_64x64x16"  64x64x16, 4 coils, 16 kz x 4 x 1024 stack of spirals
+           "toep3d_256x256x32"  256x256x32, 4 coils, 32 kz x 16 x 4096 (Toeplitz)
     `small` shrinks the sample count for fast tests (same recipe)."""
-    seed = {"bf2d_64": 1001, "bf3d_64x64x16": 1002}.get(name, 1000) if seed is None else seed
+    seed = {"bf2d_64": 1001, "bf3d_64x64x16": 1002,
+            "toep3d_256x256x32": 1003}.get(name, 1000) if seed is None else seed
     rng = np.random.default_rng(seed)
     if name == "bf2d_64":
         ny = nx = 64
@@ -158,6 +160,26 @@ def make_case(name: str, seed: int | None = None, forward=None, small: bool = Fa
         fm_v = fm.ravel()
         dims = (nx, ny, nz)
         opts = dict(cg_num=16, fd_penalizer=1e-3, tv=True, tv_num=10, use_z=1)
+    elif name == "toep3d_256x256x32":
+        # 256x256x32, 4 coils, 32 kz partitions x 16 interleaves x 4096
+        # (small: 16x16x8, 2 coils, 8 x 2 x 128)
+        ny, nx, nz = (16, 16, 8) if small else (256, 256, 32)
+        n_part, n_il, n_s = (8, 2, 128) if small else (32, 16, 4096)
+        kx2, ky2, t2 = spiral(n_il, n_s, nx / 2 - 0.05, rng)
+        kz_levels = np.arange(-nz // 2, nz // 2, dtype=np.float32)[:n_part]
+        kx = np.tile(kx2, n_part)
+        ky = np.tile(ky2, n_part)
+        kz = np.repeat(kz_levels, kx2.size).astype(np.float32)
+        t = np.tile(t2, n_part)
+        C = 2 if small else 4
+        img = ellipse_phantom((ny, nx, nz), 8, rng)
+        fm = field_map((ny, nx, nz), rng)
+        sens = coil_maps((ny, nx, nz), C, rng).reshape(C, -1)
+        x_true = img.ravel()
+        fm_v = fm.ravel()
+        dims = (nx, ny, nz)
+        opts = dict(cg_num=20, fd_penalizer=1e-3, tv=True, tv_num=10, use_z=1, ntime_segs=8,
+                    gridOS_Q=2.0, gridOS_FH=1.5)
     else:
         raise ValueError(name)
     ix, iy, iz = grid_positions(ny, nx, nz)

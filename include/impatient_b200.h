@@ -173,6 +173,73 @@ imp_status imp_bruteforce_dir(const char *idir, const char *odir, const imp_bf_o
 imp_status imp_dataset_info(const char *idir, int *num_k, int *num_i, int *num_coil,
                             int *num_slices, int *nx, int *ny, int *nz);
 
+/* ---- Toeplitz path ------------------------------------------------------
+ * Image layout: 2-D [x][y] (y fastest), 3-D [y][x][z] (z fastest), the
+ * voxel order of the reference's ix/iy/iz files.  Q is stored as in
+ * Q_stone.file: for each segment l = 0..(int)ntime_segs one block of
+ * (2nx)(2ny)(2nz or 1) values on the 2N grid, split into re and im arrays.
+ * Every array argument may be a host or a device pointer. */
+
+typedef struct imp_toeplitz_options {
+    int cg_num;          /* CG iterations (-cg_num) */
+    int enable_fd;       /* finite-difference regularization (-reg) */
+    float fd_penalizer;  /* lambda (-fdp) */
+    int enable_tv;       /* TV reweighting passes (-tv) */
+    int tv_num;          /* TV passes (-tv_num) */
+    float tv_eps;        /* TV smoothing epsilon (1e-6 in the reference) */
+    float ntime_segs;    /* L (-ntime_segs); segments l = 0..(int)L */
+    float gridOS_Q;      /* oversampling of the Q gridding (-gridOS_Q) */
+    float gridOS_FH;     /* oversampling of the F^H d gridding (-gridOS_FH) */
+} imp_toeplitz_options;
+
+/* Defaults of main.cpp:103-444 for the Toeplitz flags. */
+void imp_toeplitz_options_default(imp_toeplitz_options *opt);
+
+/* Q_l, l = 0..L, by Kaiser-Bessel gridding of h_l(t) at 2k on the
+ * oversampled 2N grid, FFT and deapodization.
+ * replaces computeQ_GPU_Grid(), toeplitz/computeQ.cmem.cu:402-756
+ * (driven by computeQ_GPU, toeplitz/computeQ.cmem.cu:757-1028).
+ * q_r/q_i: (L+1) * (2nx)(2ny)(2nz or 1) floats each. */
+imp_status imp_toeplitz_q(imp_context *ctx, const imp_toeplitz_options *opt, float *q_r,
+                          float *q_i, const float *kx, const float *ky, const float *kz,
+                          const float *t, int num_k, int nx, int ny, int nz);
+
+/* F^H d with time segmentation and SENSE by gridding.
+ * replaces computeFH_GPU_Grid(), toeplitz/computeFH.cmem.cu:470-805
+ * (driven by computeFH_GPU, toeplitz/computeFH.cmem.cu:1188-1409).
+ * kdata, sensi: [coil][...]; fm may be NULL (zero field map). */
+imp_status imp_toeplitz_fhd(imp_context *ctx, const imp_toeplitz_options *opt, float *fhd_r,
+                            float *fhd_i, const float *kdata_r, const float *kdata_i,
+                            const float *kx, const float *ky, const float *kz, const float *t,
+                            const float *fm, const float *sensi_r, const float *sensi_i,
+                            int num_k, int num_coil, int nx, int ny, int nz);
+
+/* Toeplitz CG (with optional FD regularization and TV passes) from x = 0;
+ * x receives the iterate with the smallest residual.
+ * replaces toeplitz_recon(), toeplitz/recon.cu:1724-2191. */
+imp_status imp_toeplitz_recon(imp_context *ctx, const imp_toeplitz_options *opt, float *x_r,
+                              float *x_i, const float *fhd_r, const float *fhd_i,
+                              const float *q_r, const float *q_i, const float *t, int num_k,
+                              const float *fm, const float *sensi_r, const float *sensi_i,
+                              int num_coil, int nx, int ny, int nz);
+
+/* One application of A^H A p (+ lambda D^H D p when enable_fd), the operator
+ * inside each Toeplitz CG iteration (toeplitz/recon.cu:598-840 with
+ * DHWD at W = 1).  For tests and custom solvers. */
+imp_status imp_toeplitz_apply(imp_context *ctx, const imp_toeplitz_options *opt, float *out_r,
+                              float *out_i, const float *p_r, const float *p_i,
+                              const float *q_r, const float *q_i, const float *t, int num_k,
+                              const float *fm, const float *sensi_r, const float *sensi_i,
+                              int num_coil, int nx, int ny, int nz);
+
+/* Directory-level drop-in of toeplitz(idir, ...) (main_mri.cuh:97-108,
+ * main_mri.cu:207-630): Q by gridding, by direct evaluation (direct != 0)
+ * or read from Qdir/Q_stone.file (reuseQ != 0; Qdir NULL = idir), F^H d,
+ * Toeplitz CG; writes idir/Q_stone.file (writeQ != 0), idir/FhD.file and
+ * idir/out.file as raw float32 [re x N][im x N]. */
+imp_status imp_toeplitz_dir(const char *idir, const imp_toeplitz_options *opt, int direct,
+                            int gpu_id, int reuseQ, const char *Qdir, int writeQ);
+
 /* The mriSolver command line (main.cpp:103-444) as a library call: same
  * flags, defaults and exit codes (0 ok, 1 error). */
 int imp_mrisolver_main(int argc, char **argv);
