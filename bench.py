@@ -345,6 +345,176 @@ def run_ours(args, ws, rank, local):
     return 0
 
 
+# ------------------------------------------------------------- Toeplitz --
+
+TOEP = "toep3d_256x256x32"
+TOEP_METRIC = ("s/recon (Toeplitz 3-D, 256x256x32, 4 coils, M=2.1M, L=8, Q at OS 2, "
+               "20 CG x 10 TV)")
+
+
+def toep_model_bytes(N, G, C, L1):
+    """Algorithmic HBM bytes of one A^H A application: per (coil, segment) the
+    Qf_l read (8G) and one read + write of the 2N grid per FFT (2 x 16G), the
+    image-side passes (16N), plus the sensitivities (8CN) and CG vectors (48N)."""
+    return C * L1 * (8 * G + 32 * G) + C * L1 * 16 * N + 8 * C * N + 48 * N
+
+
+def toep_cpu_sample(G_shape, C, L1, applies):
+    """Project CPU restatement (not reference code: the reference has no CPU
+    Toeplitz path) of one F^H F_l application on the 2N grid with scipy's
+    multithreaded FFT, extrapolated to C (L+1) per A^H A and `applies` per recon."""
+    import scipy.fft as sf
+    rng = np.random.default_rng(0)
+    n = tuple(s // 2 for s in G_shape)
+    img = (rng.standard_normal(n) + 1j * rng.standard_normal(n)).astype(np.complex64)
+    qf = (rng.standard_normal(G_shape) + 1j * rng.standard_normal(G_shape)).astype(np.complex64)
+    t0 = time.perf_counter()
+    big = np.zeros(G_shape, np.complex64)
+    big[tuple(slice(0, s) for s in n)] = img
+    f = sf.fftn(big, workers=-1)
+    f *= qf
+    out = sf.ifftn(f, workers=-1)[tuple(slice(0, s) for s in n)]
+    dt = time.perf_counter() - t0
+    del out
+    return dt * C * L1 * applies, dt
+
+
+def run_toeplitz(args, ws, rank, local):
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from impatient_mri_b200 import synth
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = pkg.Context(local)
+    case = synth.make_case(TOEP, seed=1003 + rank)
+    o = case["opts"]
+    M, N, C = case["M"], case["N"], case["num_coil"]
+    nx, ny, nz = case["dims"]
+    L1 = o["ntime_segs"] + 1
+    G = 8 * N
+    rng = np.random.default_rng(11 + rank)
+    # k-space values: complex Gaussian at the phantom's mean k-space power (the
+    # exact simulation, 2.1M x 2.1M x 4 NUDFT pairs, is not part of the step and
+    # the Toeplitz timing does not depend on the values)
+    kd = ((rng.standard_normal((C, M)) + 1j * rng.standard_normal((C, M)))
+          * np.sqrt(np.mean(np.abs(case["x_true"]) ** 2) * N / 2)).astype(np.complex64)
+    f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32))
+    H = {k: f32(case[k]) for k in ("kx", "ky", "kz", "t", "fm")}
+    H["sr"], H["si"] = f32(case["sens"].real.ravel()), f32(case["sens"].imag.ravel())
+    H["yr"], H["yi"] = f32(kd.real.ravel()), f32(kd.imag.ravel())
+    D = {k: v.to(dev) for k, v in H.items()}
+    opts = pkg.toeplitz_options(cg_num=o["cg_num"], fd_penalizer=o["fd_penalizer"], tv=o["tv"],
+                                tv_num=o["tv_num"], ntime_segs=o["ntime_segs"],
+                                gridOS_Q=o["gridOS_Q"], gridOS_FH=o["gridOS_FH"])
+
+    def alloc(where):
+        mk = (lambda n: torch.zeros(n, device=dev)) if where == "dev" else (
+            lambda n: torch.zeros(n).pin_memory())
+        return dict(qr=mk(L1 * G), qi=mk(L1 * G), fr=mk(N), fi=mk(N), xr=mk(N), xi=mk(N))
+
+    def recon(src, out, ev=None):
+        """Steps 1-3 of the reference's toeplitz(): Q by gridding, F^H d, CG."""
+        if ev: ev[0].record()
+        pkg.toeplitz_q(ctx, opts, out["qr"], out["qi"], src["kx"], src["ky"], src["kz"],
+                       src["t"], M, nx, ny, nz)
+        if ev: ev[1].record()
+        pkg.toeplitz_fhd(ctx, opts, out["fr"], out["fi"], src["yr"], src["yi"], src["kx"],
+                         src["ky"], src["kz"], src["t"], src["fm"], src["sr"], src["si"], M, C,
+                         nx, ny, nz)
+        if ev: ev[2].record()
+        pkg.toeplitz_recon(ctx, opts, out["xr"], out["xi"], out["fr"], out["fi"], out["qr"],
+                           out["qi"], src["t"], M, src["fm"], src["sr"], src["si"], C, nx, ny, nz)
+        if ev: ev[3].record()
+
+    B = alloc("dev")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        recon(D, B)
+    torch.cuda.synchronize()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    launches = 0
+    barrier(ws)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            flush.fill_(float(s))
+            recon(D, B, evs[s])
+            launches += ctx.launch_count()
+    torch.cuda.synchronize()
+    barrier(ws)
+    parts = np.array([[e[i].elapsed_time(e[i + 1]) for i in range(3)] for e in evs])
+    step_ms = parts.sum(1)
+    value = max_over_ranks(float(step_ms.sum()) / 1e3, ws) / (args.steps * ws)
+
+    # end to end: the same calls with pinned host buffers
+    Hb = alloc("host")
+    Hs = {k: v.pin_memory() for k, v in H.items()}
+    nb = lambda *ks: sum(Hs[k].numel() * 4 for k in ks)
+    q_bytes, f_bytes, x_bytes = 2 * L1 * G * 4, 2 * N * 4, 2 * N * 4
+    # inputs of the three calls (the trajectory is staged by each call that reads
+    # it), plus Q and F^H d going back in for the CG
+    h2d = (nb("kx", "ky", "kz", "t") + nb("kx", "ky", "kz", "t", "fm", "sr", "si", "yr", "yi")
+           + nb("t", "fm", "sr", "si") + q_bytes + f_bytes)
+    d2h = q_bytes + f_bytes + x_bytes  # Q, F^H d and the image come back
+    recon(Hs, Hb)
+    e2e = []
+    barrier(ws)
+    for s in range(args.steps):
+        flush.fill_(float(s))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        recon(Hs, Hb)
+        e2e.append(time.perf_counter() - t0)
+    barrier(ws)
+    e2e_value = max_over_ranks(float(sum(e2e)), ws) / (args.steps * ws)
+
+    applies = o["tv_num"] * (o["cg_num"] + 1)
+    cg_ms = float(np.mean(parts[:, 2]))
+    per_apply_s = cg_ms / 1e3 / applies
+    model = toep_model_bytes(N, G, C, L1)
+    achieved = model / per_apply_s / 1e9
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (
+        ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    out = {
+        "metric": TOEP_METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value * 1e3 * ws, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded trajectory/phantom/coils/field map; Gaussian k-space values)",
+        "config": {"workload": f"{TOEP}: 256x256x32, 4 coils, 32 kz x 16 x 4096 (M=2097152), "
+                               f"L=8, gridOS_Q 2.0, gridOS_FH 1.5, cg_num 20, TV 10 passes, "
+                               f"lambda 1e-3",
+                   "l2": "flushed (256 MiB write) before every timed step; grids exceed L2",
+                   "parallelism": f"replicas x{ws}"},
+        "breakdown_ms": {"q": float(np.mean(parts[:, 0])), "fhd": float(np.mean(parts[:, 1])),
+                         "cg": cg_ms},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "kernel": "A^H A application inside the CG (pad, cuFFT, x Qf_l, cuFFT, "
+                               "crop + coil sum, CG update), per application",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
+                     "algorithmic_bytes_per_apply": model, "apply_ms": per_apply_s * 1e3,
+                     "applies_per_recon": applies},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        v, dt = toep_cpu_sample((2 * ny, 2 * nx, 2 * nz), C, L1, applies)
+        out["cpu_baseline"] = {
+            "value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": (f"project CPU restatement (the reference has no CPU Toeplitz code): one "
+                       f"F^H F_l (pad, scipy FFT, x Qf, IFFT, crop) on the 512x512x64 grid "
+                       f"({dt:.2f} s), x{C * L1} per A^H A, x{applies} per recon; gridding "
+                       f"of Q and F^H d not counted")}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
 def run_nudft_only(args, local):
     """Forward + adjoint NUDFT applies of the benchmark geometry through the
     operator C-ABI (the small command the kernel profiles are taken on)."""
@@ -382,6 +552,8 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, TOEP],
+                    help="bf3d_64x64x16 (default, the headline) or the Toeplitz 3-D case")
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     try:
@@ -389,6 +561,8 @@ def main() -> int:
             return run_nudft_only(args, local)
         if args.impl == "reference":
             return run_reference(args, ws, rank)
+        if args.workload == TOEP:
+            return run_toeplitz(args, ws, rank, local)
         return run_ours(args, ws, rank, local)
     finally:
         if ws > 1:

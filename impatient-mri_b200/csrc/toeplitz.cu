@@ -542,6 +542,33 @@ void ToepSolver::release() {
 cudaError_t ToepSolver::setup(const ToepConfig &cfg, const float *t, const float *fm,
                               const float *sensi_r, const float *sensi_i, unsigned *dev_err,
                               cudaStream_t st) {
+    // Same sizes and stream: keep buffers, FFT plans and (same CG terms) the
+    // captured iteration graph; only the per-call inputs are refreshed.
+    const bool same_shape = dots_ && st == st_ && cfg.nx == cfg_.nx && cfg.ny == cfg_.ny &&
+                            cfg.nz == cfg_.nz && cfg.C == cfg_.C && cfg.M == cfg_.M &&
+                            (int)cfg.ntime_segs == L_;
+    if (same_shape) {
+        if (g_iter_ && (cfg.fd != cfg_.fd || cfg.lambda != cfg_.lambda ||
+                        cfg.use_graphs != cfg_.use_graphs)) {
+            cudaGraphExecDestroy(g_iter_);
+            g_iter_ = nullptr;
+        }
+        cfg_ = cfg;
+        err_ = dev_err;
+        float tb[2] = {0.f, 0.f};
+        T_TRY(cudaMemcpyAsync(&tb[0], t, sizeof(float), cudaMemcpyDeviceToHost, st));
+        T_TRY(cudaMemcpyAsync(&tb[1], t + cfg.M - 1, sizeof(float), cudaMemcpyDeviceToHost, st));
+        T_TRY(cudaStreamSynchronize(st));
+        tau_ = cfg.ntime_segs > 0.f ? (tb[1] - tb[0]) / cfg.ntime_segs : (tb[1] - tb[0]);
+        t0_ = tb[0];
+        const int L1 = L_ + 1, C = cfg.C;
+        T_TRY(cudaMemcpyAsync(t_, t, sizeof(float) * cfg.M, cudaMemcpyDeviceToDevice, st));
+        k_pack_sens_c<<<gridn((size_t)C * N_), kVB, 0, st>>>(sens_, sensi_r, sensi_i,
+                                                            (size_t)C * N_);
+        k_eph<<<gridn((size_t)L1 * N_), kVB, 0, st>>>(eph_, fm, N_, L1, tau_, t0_);
+        launches_ = 2;
+        return cudaGetLastError();
+    }
     release();
     cfg_ = cfg;
     st_ = st;
@@ -637,7 +664,7 @@ cudaError_t ToepSolver::compute_q(const float *kx, const float *ky, const float 
                                              q_out_i ? q_out_i + (size_t)l * G2_ : nullptr, G2_);
         T_TRY(cudaGetLastError());
         T_FFT(cufftExecC2C(plan1_, qf_l, qf_l, CUFFT_FORWARD));
-        launches_ += 4;
+        launches_ += 2;  // own kernels only (cuFFT launches are not counted)
     }
     return cudaStreamSynchronize(st_);
 }
@@ -650,7 +677,7 @@ cudaError_t ToepSolver::load_q(const float *q_r, const float *q_i) {
                                               cfg_.nz > 1, qf_l, G2_);
         T_TRY(cudaGetLastError());
         T_FFT(cufftExecC2C(plan1_, qf_l, qf_l, CUFFT_FORWARD));
-        launches_ += 2;
+        launches_ += 1;
     }
     return cudaStreamSynchronize(st_);
 }
@@ -676,11 +703,12 @@ cudaError_t ToepSolver::compute_fhd(const float *kx, const float *ky, const floa
             k_fh_post<<<gridn(N_), kVB, 0, st_>>>(grid_, g, nvd, N_, sens_ + (size_t)c * N_,
                                                  eph_ + (size_t)l * N_, fhd_);
             T_TRY(cudaGetLastError());
-            launches_ += 3;
+            launches_ += 2;
         }
     if (fhd_r) {
         k_c2soa<<<gridn(N_), kVB, 0, st_>>>(fhd_r, fhd_i, fhd_, N_);
         T_TRY(cudaGetLastError());
+        ++launches_;
     }
     return cudaStreamSynchronize(st_);
 }
@@ -748,7 +776,7 @@ cudaError_t ToepSolver::solve(const float *fhd_r, const float *fhd_i, float *x_r
     k_t_norm_finish<<<1, kVB, 0, st_>>>(dots_);
     T_TRY(cudaGetLastError());
     launches_ += 4;
-    const int iter_launches = 5 * (L_ + 1) + 4;
+    const int iter_launches = 3 * (L_ + 1) + 4;  // own kernels of one CG iteration
     if (cfg_.use_graphs && !g_iter_) T_TRY(capture_graph(st_, &g_iter_, &ToepSolver::cg_iteration, this));
     for (int tv_i = 0; tv_i < std::max(cfg_.tv ? cfg_.tv_num : 1, 1); ++tv_i) {
         if (tv_i != 0) {
