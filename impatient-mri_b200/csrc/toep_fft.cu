@@ -1,0 +1,711 @@
+// Pruned, fused FFT engine for the Toeplitz F^H F (see toep_fft.cuh).
+//
+// Line transforms of length n <= 32 run in one register pass; longer ones as
+// n = R1 * R2 (R1, R2 <= 32) in two passes over shared memory:
+//   pass 1 ("stride"):  for each j1, an R2-point DFT over j2 of x[j1 + R1 j2],
+//                       times w_n^{j1 k2}, stored back at j1 + R1 k2;
+//   pass 2 ("contig"):  for each k2, an R1-point DFT over the slots
+//                       k1 + R1 k2, which then hold X[k2 + R2 k1].
+// The inverse runs the two passes in the opposite order (contig with the
+// conjugate twiddle after the DFT, then stride) and returns natural order, so
+// the forward's permuted "slot" order never has to be undone in memory.
+#include "common.cuh"
+#include "toep_fft.cuh"
+
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace imp {
+
+namespace cg = cooperative_groups;
+
+namespace {
+
+constexpr int kTwN = 2048;      // twiddle table: exp(-2 pi i j / kTwN)
+constexpr int kPlaneThreads = 512;
+
+__host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n >> 1); }
+
+__host__ __device__ constexpr int rev_bits(int i, int bits) {
+    int r = 0;
+    for (int b = 0; b < bits; ++b) r |= ((i >> b) & 1) << (bits - 1 - b);
+    return r;
+}
+
+// n = R1 * R2 with R1 = 1 for n <= 32, else R1 = 2^floor(log2(n) / 2).
+__host__ __device__ constexpr int split_r1(int n) { return n <= 32 ? 1 : 1 << (ilog2c(n) / 2); }
+
+constexpr int kTwLg = 11;      // log2(kTwN)
+
+// Slot of natural frequency k after a forward transform of length n = r1 r2
+// (lr2 = log2 r2).
+__device__ __forceinline__ int slot_of(int k, int r1, int lr2) {
+    return (k >> lr2) + r1 * (k & ((1 << lr2) - 1));
+}
+
+// w_n^e (conjugated when inv), n = 2^lg <= kTwN.
+__device__ __forceinline__ float2 wn(const float2 *__restrict__ tw, int e, int lg, bool inv) {
+    float2 w = __ldg(&tw[(e & ((1 << lg) - 1)) << (kTwLg - lg)]);
+    if (inv) w.y = -w.y;
+    return w;
+}
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+
+// cos / sin of a compile-time angle (radians, |x| <= 2 pi) by Taylor series,
+// evaluated by the compiler; used for the butterfly constants of the register
+// DFTs so that they become immediates.
+__host__ __device__ constexpr double taylor_sin(double x) {
+    double term = x, sum = x;
+    for (int k = 1; k < 30; ++k) {
+        term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+__host__ __device__ constexpr double taylor_cos(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int k = 1; k < 30; ++k) {
+        term *= -x * x / ((2.0 * k - 1.0) * (2.0 * k));
+        sum += term;
+    }
+    return sum;
+}
+
+// Butterflies of twiddle index K in the stage of half-width HALF, then the
+// rest of the network (radix-2 DIT on bit-reversed registers).
+template <int R, int HALF, int K, bool INV>
+__device__ __forceinline__ void dit_stage(float2 (&v)[R]) {
+    if constexpr (HALF < R) {
+        if constexpr (K < HALF) {
+            // w = exp(-+ 2 pi i K / (2 HALF))
+            constexpr double ang = -3.14159265358979323846264338327950288 * K / HALF;
+            constexpr float wc = (float)taylor_cos(ang);
+            constexpr float ws = (float)(INV ? -taylor_sin(ang) : taylor_sin(ang));
+#pragma unroll
+            for (int i = 0; i < R; i += 2 * HALF) {
+                const float2 a = v[i + K];
+                float2 b = v[i + K + HALF];
+                if constexpr (K == 0) {
+                } else if constexpr (2 * K == HALF) {  // -i (forward) / +i (inverse)
+                    b = INV ? make_float2(-b.y, b.x) : make_float2(b.y, -b.x);
+                } else {
+                    b = make_float2(b.x * wc - b.y * ws, b.x * ws + b.y * wc);
+                }
+                v[i + K] = make_float2(a.x + b.x, a.y + b.y);
+                v[i + K + HALF] = make_float2(a.x - b.x, a.y - b.y);
+            }
+            dit_stage<R, HALF, K + 1, INV>(v);
+        } else {
+            dit_stage<R, 2 * HALF, 0, INV>(v);
+        }
+    }
+}
+
+// In-register DFT of R points, natural order in and out (radix-2 DIT; the
+// bit reversal is a compile-time register renaming).
+template <int R, bool INV>
+__device__ __forceinline__ void dft(float2 (&v)[R], const float2 *__restrict__) {
+    constexpr int LG = ilog2c(R);
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+        const int j = rev_bits(i, LG);
+        if (j > i) {
+            const float2 t = v[i];
+            v[i] = v[j];
+            v[j] = t;
+        }
+    }
+    dit_stage<R, 1, 0, INV>(v);
+}
+
+// A set of 2^nl_lg lines in shared memory: line l starts at
+// (l >> lpb_lg) * bstride + (l & (2^lpb_lg - 1)) * lstride; element e of a
+// line is at start + e * es.
+struct Lines {
+    int nl_lg, lpb_lg, lstride, bstride, es;
+};
+
+__device__ __forceinline__ int line_base(const Lines &L, int l) {
+    return (l >> L.lpb_lg) * L.bstride + (l & ((1 << L.lpb_lg) - 1)) * L.lstride;
+}
+
+// Stride pass: R = R2-point DFTs over j2 for every (line, j1); optional
+// twiddle w_n^{+-j1 k2} after the DFT.
+template <int R, bool INV>
+__device__ __forceinline__ void pass_stride(float2 *buf, const Lines L, int r1, int lgn,
+                                            bool twiddle, const float2 *__restrict__ tw) {
+    const int items = r1 << L.nl_lg;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int l = it & ((1 << L.nl_lg) - 1), j1 = it >> L.nl_lg;
+        float2 *b = buf + line_base(L, l) + j1 * L.es;
+        const int st = r1 * L.es;
+        float2 v[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = b[q * st];
+        dft<R, INV>(v, tw);
+        if (twiddle && j1 != 0) {
+#pragma unroll
+            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], wn(tw, j1 * q, lgn, INV));
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) b[q * st] = v[q];
+    }
+}
+
+// Contiguous-slot pass: R = R1-point DFTs over k1 for every (line, k2); the
+// inverse multiplies output j1 by w_n^{-j1 k2}.
+template <int R, bool INV>
+__device__ __forceinline__ void pass_contig(float2 *buf, const Lines L, int r2, int lgn,
+                                            const float2 *__restrict__ tw) {
+    const int items = r2 << L.nl_lg;
+    for (int it = threadIdx.x; it < items; it += blockDim.x) {
+        const int l = it & ((1 << L.nl_lg) - 1), k2 = it >> L.nl_lg;
+        float2 *b = buf + line_base(L, l) + R * k2 * L.es;
+        float2 v[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) v[q] = b[q * L.es];
+        dft<R, INV>(v, tw);
+        if (INV && k2 != 0) {
+#pragma unroll
+            for (int q = 1; q < R; ++q) v[q] = cmul(v[q], wn(tw, q * k2, lgn, true));
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) b[q * L.es] = v[q];
+    }
+}
+
+template <bool INV>
+__device__ __forceinline__ void run_stride(float2 *buf, const Lines L, int r1, int r2, int lgn,
+                                           bool twiddle, const float2 *__restrict__ tw) {
+    switch (r2) {
+        case 1: break;
+        case 2: pass_stride<2, INV>(buf, L, r1, lgn, twiddle, tw); break;
+        case 4: pass_stride<4, INV>(buf, L, r1, lgn, twiddle, tw); break;
+        case 8: pass_stride<8, INV>(buf, L, r1, lgn, twiddle, tw); break;
+        case 16: pass_stride<16, INV>(buf, L, r1, lgn, twiddle, tw); break;
+        default: pass_stride<32, INV>(buf, L, r1, lgn, twiddle, tw); break;
+    }
+}
+
+template <bool INV>
+__device__ __forceinline__ void run_contig(float2 *buf, const Lines L, int r1, int r2, int lgn,
+                                           const float2 *__restrict__ tw) {
+    switch (r1) {
+        case 1: break;
+        case 2: pass_contig<2, INV>(buf, L, r2, lgn, tw); break;
+        case 4: pass_contig<4, INV>(buf, L, r2, lgn, tw); break;
+        case 8: pass_contig<8, INV>(buf, L, r2, lgn, tw); break;
+        case 16: pass_contig<16, INV>(buf, L, r2, lgn, tw); break;
+        default: pass_contig<32, INV>(buf, L, r2, lgn, tw); break;
+    }
+}
+
+struct PlaneGeo {
+    int ns, nm, nf, qm, ps, rs, ncol, C;
+    int r1m, r2m, r1f, r2f;
+    int lnm, lnf, lplane, lr2m, lr2f, lps;  // log2 of nm, nf, nm*nf, r2m, r2f, ps
+};
+
+// Bounded mbarrier wait (about 2^22 polls); false when it ran out.
+__device__ __forceinline__ bool wait_bounded(uint64_t *bar, unsigned parity) {
+    for (unsigned it = 0; it < (1u << 22); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// Forward plane transform of coil c = blockIdx.y for the s-planes
+// [blockIdx.x * ps, +ps).  The padded input S_c e_l x is formed once in
+// shared memory (U); each (am, af) parity quadrant is then twiddled into the
+// work plane P, transformed, and written to b1[c][s][am][af][km][kf] in
+// natural frequency order.
+template <int VPT>
+__global__ void __launch_bounds__(kPlaneThreads) k_fwd_plane(
+    float2 *__restrict__ b1, const float2 *__restrict__ x, const float2 *__restrict__ sens,
+    const float2 *__restrict__ eph_l, PlaneGeo g, const float2 *__restrict__ tw,
+    const int *__restrict__ done) {
+    extern __shared__ float2 smem[];
+    if (done && *done) return;
+    const int plane = 1 << g.lplane;
+    const int s0 = blockIdx.x * g.ps, c = blockIdx.y;
+    const int ecta = g.ps << g.lplane;
+    const size_t N = (size_t)g.ns << g.lplane;
+    const size_t vbase = (size_t)s0 << g.lplane;
+    const int pstride = g.nm * g.rs;
+    float2 *P = smem;
+    float2 *U = smem + (size_t)g.ps * pstride;
+    const Lines rows{g.lps + g.lnm, g.lps + g.lnm, g.rs, 0, 1};
+    const Lines cols{g.lps + g.lnf, g.lnf, 1, pstride, g.rs};
+    const float2 *sc = sens + (size_t)c * N + vbase;
+    const float2 *ec = eph_l + vbase;
+    const float2 *xc = x + vbase;
+#pragma unroll
+    for (int i = 0; i < VPT; ++i) {
+        const int e = threadIdx.x + i * kPlaneThreads;
+        if (e < ecta) U[e] = cmul(cmul(__ldg(&sc[e]), __ldg(&ec[e])), __ldg(&xc[e]));
+    }
+    for (int am = 0; am < g.qm; ++am)
+        for (int af = 0; af < 2; ++af) {
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < VPT; ++i) {
+                const int e = threadIdx.x + i * kPlaneThreads;
+                if (e < ecta) {
+                    const int pp = e >> g.lplane, r = e & (plane - 1);
+                    const int m = r >> g.lnf, f = r & (g.nf - 1);
+                    float2 val = U[e];
+                    if (am) val = cmul(val, wn(tw, m, g.lnm + 1, false));
+                    if (af) val = cmul(val, wn(tw, f, g.lnf + 1, false));
+                    P[pp * pstride + m * g.rs + f] = val;
+                }
+            }
+            __syncthreads();
+            run_stride<false>(P, rows, g.r1f, g.r2f, g.lnf, true, tw);
+            __syncthreads();
+            if (g.r1f > 1) {
+                run_contig<false>(P, rows, g.r1f, g.r2f, g.lnf, tw);
+                __syncthreads();
+            }
+            if (g.nm > 1) {
+                run_stride<false>(P, cols, g.r1m, g.r2m, g.lnm, true, tw);
+                __syncthreads();
+                if (g.r1m > 1) {
+                    run_contig<false>(P, cols, g.r1m, g.r2m, g.lnm, tw);
+                    __syncthreads();
+                }
+            }
+            float2 *dst = b1 + ((size_t)c * g.ns + s0) * g.ncol + ((size_t)(am * 2 + af) << g.lplane);
+#pragma unroll
+            for (int i = 0; i < VPT; ++i) {
+                const int e = threadIdx.x + i * kPlaneThreads;
+                if (e < ecta) {
+                    const int pp = e >> g.lplane, r = e & (plane - 1);
+                    const int km = r >> g.lnf, kf = r & (g.nf - 1);
+                    const int sm = g.nm > 1 ? slot_of(km, g.r1m, g.lr2m) : 0;
+                    dst[(size_t)pp * g.ncol + r] =
+                        P[pp * pstride + sm * g.rs + slot_of(kf, g.r1f, g.lr2f)];
+                }
+            }
+        }
+}
+
+// Inverse plane transform for the s-planes [blockIdx.x * ps, +ps).  The
+// blockDim.y-wide cluster (cluster rank = blockIdx.y) splits the coils: block
+// r takes coils r, r + csize, ...  Each parity quadrant of b1 is brought into
+// the staging buffer St by bulk copies (cp.async.bulk on an mbarrier, the next
+// quadrant's copy overlapping this quadrant's transform), scattered into the
+// work plane P in slot order, inverse-transformed, twiddled, multiplied by
+// conj(S_c) and added to the block's partial sum Y.  The cluster then adds the
+// csize partial sums over distributed shared memory (block r reduces its
+// 1/csize share of the plane), applies conj(e_l) and writes (first) or
+// accumulates q.  A copy that does not complete within the bounded wait sets
+// DEV_ERR_TIMEOUT in *err and ends the block's work early.
+template <int VPT>
+__global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
+    float2 *__restrict__ q, const float2 *__restrict__ b1, const float2 *__restrict__ sens,
+    const float2 *__restrict__ eph_l, PlaneGeo g, int first, const float2 *__restrict__ tw,
+    const int *__restrict__ done, unsigned *err) {
+    extern __shared__ __align__(16) float2 smem[];
+    __shared__ __align__(8) uint64_t bar;
+    cg::cluster_group cluster = cg::this_cluster();
+    const int plane = 1 << g.lplane;
+    const int ecta = g.ps << g.lplane;
+    const int pstride = g.nm * g.rs;
+    float2 *St = smem;                                // staging, natural order [ps][plane]
+    float2 *Y = smem + ecta;                          // partial coil sum, natural order
+    float2 *P = smem + 2 * (size_t)ecta;              // FFT work plane(s), padded rows
+    const bool skip = done && *done;
+    const int rank = blockIdx.y, csize = gridDim.y;
+    const int s0 = blockIdx.x * g.ps;
+    if (!skip) {
+        const size_t N = (size_t)g.ns << g.lplane;
+        const size_t vbase = (size_t)s0 << g.lplane;
+        const Lines rows{g.lps + g.lnm, g.lps + g.lnm, g.rs, 0, 1};
+        const Lines cols{g.lps + g.lnf, g.lnf, 1, pstride, g.rs};
+        const int nquad = g.qm * 2;
+        const int my_coils = (g.C - rank + csize - 1) / csize;
+        const int nq = my_coils * nquad;
+        auto src_of = [&](int qi) {
+            const int c = rank + (qi / nquad) * csize, quad = qi % nquad;
+            return b1 + ((size_t)c * g.ns + s0) * g.ncol + ((size_t)quad << g.lplane);
+        };
+        auto issue = [&](int qi) {
+            const float2 *src = src_of(qi);
+            mbar_arrive_expect_tx(&bar, (unsigned)(ecta * sizeof(float2)));
+            for (int pp = 0; pp < g.ps; ++pp)
+                bulk_g2s(St + (size_t)pp * plane, src + (size_t)pp * g.ncol,
+                         (unsigned)(plane * sizeof(float2)), &bar);
+        };
+        if (threadIdx.x == 0) {
+            mbar_init(&bar, 1);
+            fence_mbar_init();
+        }
+        for (int e = threadIdx.x; e < ecta; e += kPlaneThreads) Y[e] = make_float2(0.f, 0.f);
+        __syncthreads();
+        if (threadIdx.x == 0 && nq > 0) issue(0);
+        unsigned phase = 0;
+        for (int qi = 0; qi < nq; ++qi) {
+            const bool ok = wait_bounded(&bar, phase);
+            phase ^= 1u;
+            if (__syncthreads_or(!ok)) {
+                if (threadIdx.x == 0) {
+                    if (err) atomicOr(err, DEV_ERR_TIMEOUT);
+                    wait_bounded(&bar, phase ^ 1u);  // the copy still in flight, bounded
+                }
+                break;
+            }
+            const int c = rank + (qi / nquad) * csize, quad = qi % nquad;
+            const int am = quad >> 1, af = quad & 1;
+#pragma unroll
+            for (int i = 0; i < VPT; ++i) {
+                const int e = threadIdx.x + i * kPlaneThreads;
+                if (e < ecta) {
+                    const int pp = e >> g.lplane, r = e & (plane - 1);
+                    const int km = r >> g.lnf, kf = r & (g.nf - 1);
+                    const int sm = g.nm > 1 ? slot_of(km, g.r1m, g.lr2m) : 0;
+                    P[pp * pstride + sm * g.rs + slot_of(kf, g.r1f, g.lr2f)] = St[e];
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0 && qi + 1 < nq) {
+                fence_proxy_async_smem();  // St reads done before the next async write
+                issue(qi + 1);
+            }
+            if (g.nm > 1) {
+                if (g.r1m > 1) {
+                    run_contig<true>(P, cols, g.r1m, g.r2m, g.lnm, tw);
+                    __syncthreads();
+                }
+                run_stride<true>(P, cols, g.r1m, g.r2m, g.lnm, false, tw);
+                __syncthreads();
+            }
+            if (g.r1f > 1) {
+                run_contig<true>(P, rows, g.r1f, g.r2f, g.lnf, tw);
+                __syncthreads();
+            }
+            run_stride<true>(P, rows, g.r1f, g.r2f, g.lnf, false, tw);
+            __syncthreads();
+            const float2 *sc = sens + (size_t)c * N + vbase;
+#pragma unroll
+            for (int i = 0; i < VPT; ++i) {
+                const int e = threadIdx.x + i * kPlaneThreads;
+                if (e < ecta) {
+                    const int pp = e >> g.lplane, r = e & (plane - 1);
+                    const int m = r >> g.lnf, f = r & (g.nf - 1);
+                    float2 val = P[pp * pstride + m * g.rs + f];
+                    if (am) val = cmul(val, wn(tw, m, g.lnm + 1, true));
+                    if (af) val = cmul(val, wn(tw, f, g.lnf + 1, true));
+                    Y[e] = cadd(Y[e], cmulc(__ldg(&sc[e]), val));
+                }
+            }
+        }
+    }
+    cluster.sync();
+    if (!skip) {
+        const size_t vbase = (size_t)s0 << g.lplane;
+        const int share = (ecta + csize - 1) / csize;
+        const int e0 = rank * share, e1 = min(ecta, e0 + share);
+        for (int e = e0 + threadIdx.x; e < e1; e += kPlaneThreads) {
+            float2 sum = make_float2(0.f, 0.f);
+            for (int r = 0; r < csize; ++r) sum = cadd(sum, cluster.map_shared_rank(Y, r)[e]);
+            const size_t v = vbase + e;
+            float2 out = cmulc(eph_l[v], sum);
+            if (!first) out = cadd(out, q[v]);
+            q[v] = out;
+        }
+    }
+    cluster.sync();  // no block leaves while another still reads its Y
+}
+
+// Slow axis for the spectrum columns [blockIdx.x * W, +W) of every coil:
+// per s-parity a, forward FFT along s of x[s] w_2ns^{a s}, x Qf_l (parity a),
+// inverse FFT, times w_2ns^{-a s}; the two parities are summed in registers
+// and written back in place.  blockDim = W * R1: thread (w, j1).
+constexpr int kSlowThreads = 256;
+
+template <int NS>
+__global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
+    float2 *__restrict__ b1, const float2 *__restrict__ qf2, int C, int ncol, int W,
+    const float2 *__restrict__ tw, const int *__restrict__ done) {
+    constexpr int R1 = split_r1(NS), R2 = NS / R1;
+    constexpr int LNS = ilog2c(NS);
+    extern __shared__ float2 E[];       // [NS][W] work
+    float2 *Y = E + NS * W;             // [NS][W] parity sum (each thread owns its slots)
+    if (done && *done) return;
+    const int col0 = blockIdx.x * W;
+    const int lw = __ffs(W) - 1;
+    const int w = threadIdx.x & (W - 1), j1 = threadIdx.x >> lw;
+    const size_t per_coil = (size_t)NS * ncol;
+    for (int c = 0; c < C; ++c) {
+        float2 *bc = b1 + (size_t)c * per_coil + col0;
+        for (int a = 0; a < 2; ++a) {
+            {
+                float2 v[R2];
+#pragma unroll
+                for (int q = 0; q < R2; ++q) {
+                    const int s = j1 + R1 * q;
+                    float2 xv = bc[(size_t)s * ncol + w];
+                    if (a) xv = cmul(xv, wn(tw, s, LNS + 1, false));
+                    v[q] = xv;
+                }
+                dft<R2, false>(v, tw);
+                if (j1 != 0) {
+#pragma unroll
+                    for (int q = 1; q < R2; ++q) v[q] = cmul(v[q], wn(tw, j1 * q, LNS, false));
+                }
+#pragma unroll
+                for (int q = 0; q < R2; ++q) E[(j1 + R1 * q) * W + w] = v[q];
+            }
+            __syncthreads();
+            for (int it = threadIdx.x; it < W * R2; it += blockDim.x) {
+                const int w2 = it & (W - 1), k2 = it >> lw;
+                float2 z[R1];
+#pragma unroll
+                for (int k1 = 0; k1 < R1; ++k1) z[k1] = E[(k1 + R1 * k2) * W + w2];
+                dft<R1, false>(z, tw);
+#pragma unroll
+                for (int k1 = 0; k1 < R1; ++k1) {
+                    const int k = k2 + R2 * k1;
+                    z[k1] = cmul(z[k1], __ldg(&qf2[(size_t)(a * NS + k) * ncol + col0 + w2]));
+                }
+                dft<R1, true>(z, tw);
+                if (k2 != 0) {
+#pragma unroll
+                    for (int j = 1; j < R1; ++j) z[j] = cmul(z[j], wn(tw, j * k2, LNS, true));
+                }
+#pragma unroll
+                for (int j = 0; j < R1; ++j) E[(j + R1 * k2) * W + w2] = z[j];
+            }
+            __syncthreads();
+            {
+                float2 v[R2];
+#pragma unroll
+                for (int q = 0; q < R2; ++q) v[q] = E[(j1 + R1 * q) * W + w];
+                dft<R2, true>(v, tw);
+#pragma unroll
+                for (int q = 0; q < R2; ++q) {
+                    float2 xv = v[q];
+                    const int o = (j1 + R1 * q) * W + w;
+                    if (a) {
+                        xv = cmul(xv, wn(tw, j1 + R1 * q, LNS + 1, true));
+                        Y[o] = cadd(Y[o], xv);
+                    } else {
+                        Y[o] = xv;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+#pragma unroll 4
+        for (int q = 0; q < R2; ++q) bc[(size_t)(j1 + R1 * q) * ncol + w] = Y[(j1 + R1 * q) * W + w];
+    }
+}
+
+__global__ void k_qf_perm(float2 *__restrict__ qf2, const float2 *__restrict__ qf, int ns, int nm,
+                          int nf, int qm, int ncol, float scale) {
+    const int nmf = qm == 2 ? 2 * nm : 1;
+    const size_t total = (size_t)2 * ns * nmf * 2 * nf;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total;
+         idx += (size_t)gridDim.x * blockDim.x) {
+        const int kfn = (int)(idx % (2 * nf));
+        const size_t t = idx / (2 * nf);
+        const int kmn = (int)(t % nmf);
+        const int ksn = (int)(t / nmf);
+        const int as = ksn & 1, ks = ksn >> 1, af = kfn & 1, kf = kfn >> 1;
+        const int am = qm == 2 ? (kmn & 1) : 0, km = qm == 2 ? (kmn >> 1) : 0;
+        const int col = ((am * 2 + af) * nm + km) * nf + kf;
+        const float2 v = qf[idx];
+        qf2[(size_t)(as * ns + ks) * ncol + col] = make_float2(v.x * scale, v.y * scale);
+    }
+}
+
+bool pow2(int n) { return n >= 1 && (n & (n - 1)) == 0; }
+
+template <int VPT>
+cudaError_t set_plane_smem(size_t fwd_bytes, size_t inv_bytes) {
+    cudaError_t e = cudaFuncSetAttribute(
+        k_fwd_plane<VPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_bytes);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_inv_plane<VPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)inv_bytes);
+}
+
+template <int NS>
+cudaError_t set_slow_smem(size_t bytes) {
+    return cudaFuncSetAttribute(k_slow<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)bytes);
+}
+
+PlaneGeo geo_of(const ToepFftPlan &p) {
+    PlaneGeo g;
+    g.ns = p.ns;
+    g.nm = p.nm;
+    g.nf = p.nf;
+    g.qm = p.qm;
+    g.ps = p.ps;
+    g.rs = p.rs;
+    g.ncol = p.ncol;
+    g.C = p.C;
+    g.r1m = split_r1(p.nm);
+    g.r2m = p.nm / g.r1m;
+    g.r1f = split_r1(p.nf);
+    g.r2f = p.nf / g.r1f;
+    g.lnm = ilog2c(p.nm);
+    g.lnf = ilog2c(p.nf);
+    g.lplane = g.lnm + g.lnf;
+    g.lr2m = ilog2c(g.r2m);
+    g.lr2f = ilog2c(g.r2f);
+    g.lps = ilog2c(p.ps);
+    return g;
+}
+
+}  // namespace
+
+bool toep_fft_plan(int ns, int nm, int nf, int C, ToepFftPlan *plan) {
+    if (!pow2(ns) || !pow2(nm) || !pow2(nf) || ns < 2 || nf < 2 || ns > 1024 || nf > 1024 ||
+        nm > 1024 || (size_t)nm * nf > 16384 || C < 1)
+        return false;
+    ToepFftPlan p;
+    p.ns = ns;
+    p.nm = nm;
+    p.nf = nf;
+    p.qm = nm > 1 ? 2 : 1;
+    p.C = C;
+    const int plane = nm * nf;
+    p.ps = std::max(1, std::min(ns, 8192 / plane));
+    p.rs = nf + 1;
+    const int ecta = p.ps * plane;
+    p.vpt = std::max(1, ecta / kPlaneThreads);
+    p.ncol = p.qm * 2 * plane;
+    const int r1 = split_r1(ns);
+    p.W = std::max(1, std::min(p.ncol, std::min(4096 / ns, kSlowThreads / r1)));
+    p.smem_plane = (size_t)p.ps * nm * p.rs * sizeof(float2) + (size_t)ecta * sizeof(float2);
+    p.smem_inv = p.smem_plane + (size_t)ecta * sizeof(float2);
+    p.smem_slow = 2 * (size_t)ns * p.W * sizeof(float2);
+    constexpr size_t kMaxSmem = 227 * 1024 - 64;  // room for the static mbarrier
+    if (p.smem_inv > kMaxSmem || p.smem_slow > kMaxSmem) return false;
+    for (int cs = std::min(C, 8); cs >= 1; --cs)
+        if (C % cs == 0) {
+            p.csize = cs;
+            break;
+        }
+    cudaError_t e;
+    switch (p.vpt) {
+        case 1: e = set_plane_smem<1>(p.smem_plane, p.smem_inv); break;
+        case 2: e = set_plane_smem<2>(p.smem_plane, p.smem_inv); break;
+        case 4: e = set_plane_smem<4>(p.smem_plane, p.smem_inv); break;
+        case 8: e = set_plane_smem<8>(p.smem_plane, p.smem_inv); break;
+        case 16: e = set_plane_smem<16>(p.smem_plane, p.smem_inv); break;
+        case 32: e = set_plane_smem<32>(p.smem_plane, p.smem_inv); break;
+        default: return false;
+    }
+    if (e != cudaSuccess) return false;
+    switch (ns) {
+        case 2: e = set_slow_smem<2>(p.smem_slow); break;
+        case 4: e = set_slow_smem<4>(p.smem_slow); break;
+        case 8: e = set_slow_smem<8>(p.smem_slow); break;
+        case 16: e = set_slow_smem<16>(p.smem_slow); break;
+        case 32: e = set_slow_smem<32>(p.smem_slow); break;
+        case 64: e = set_slow_smem<64>(p.smem_slow); break;
+        case 128: e = set_slow_smem<128>(p.smem_slow); break;
+        case 256: e = set_slow_smem<256>(p.smem_slow); break;
+        case 512: e = set_slow_smem<512>(p.smem_slow); break;
+        default: e = set_slow_smem<1024>(p.smem_slow); break;
+    }
+    if (e != cudaSuccess) return false;
+    *plan = p;
+    return true;
+}
+
+cudaError_t toep_fft_twiddles(float2 **tw) {
+    std::vector<float2> h(kTwN);
+    for (int j = 0; j < kTwN; ++j) {
+        const double a = -2.0 * 3.14159265358979323846264338327950288 * j / kTwN;
+        h[j] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    cudaError_t e = cudaMalloc(tw, sizeof(float2) * kTwN);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*tw, h.data(), sizeof(float2) * kTwN, cudaMemcpyHostToDevice);
+}
+
+cudaError_t toep_fft_qf(const ToepFftPlan &p, float2 *qf2_l, const float2 *qf_l, float scale,
+                        cudaStream_t st) {
+    const size_t total = (size_t)2 * p.ns * p.ncol;
+    const int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 16);
+    k_qf_perm<<<blocks, 256, 0, st>>>(qf2_l, qf_l, p.ns, p.nm, p.nf, p.qm, p.ncol, scale);
+    return cudaGetLastError();
+}
+
+cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
+                             const float2 *sens, const float2 *eph_l, float2 *b1,
+                             const float2 *qf2_l, int first, const int *done, const float2 *tw,
+                             unsigned *err, cudaStream_t st) {
+    const PlaneGeo g = geo_of(p);
+    const dim3 ga(p.ns / p.ps, p.C);
+#define IMP_PLANE_CASE(V)                                                                   \
+    case V:                                                                                 \
+        k_fwd_plane<V><<<ga, kPlaneThreads, p.smem_plane, st>>>(b1, x, sens, eph_l, g, tw,  \
+                                                                done);                      \
+        break;
+    switch (p.vpt) {
+        IMP_PLANE_CASE(1)
+        IMP_PLANE_CASE(2)
+        IMP_PLANE_CASE(4)
+        IMP_PLANE_CASE(8)
+        IMP_PLANE_CASE(16)
+        IMP_PLANE_CASE(32)
+        default: return cudaErrorInvalidValue;
+    }
+#undef IMP_PLANE_CASE
+    const int r1 = split_r1(p.ns);
+    const int blocks = p.ncol / p.W;
+    const int threads = p.W * r1;
+#define IMP_SLOW_CASE(NSV)                                                                 \
+    case NSV:                                                                              \
+        k_slow<NSV><<<blocks, threads, p.smem_slow, st>>>(b1, qf2_l, p.C, p.ncol, p.W, tw, \
+                                                          done);                           \
+        break;
+    switch (p.ns) {
+        IMP_SLOW_CASE(2)
+        IMP_SLOW_CASE(4)
+        IMP_SLOW_CASE(8)
+        IMP_SLOW_CASE(16)
+        IMP_SLOW_CASE(32)
+        IMP_SLOW_CASE(64)
+        IMP_SLOW_CASE(128)
+        IMP_SLOW_CASE(256)
+        IMP_SLOW_CASE(512)
+        IMP_SLOW_CASE(1024)
+        default: return cudaErrorInvalidValue;
+    }
+#undef IMP_SLOW_CASE
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(p.ns / p.ps, p.csize);
+    cfg.blockDim = dim3(kPlaneThreads);
+    cfg.dynamicSmemBytes = p.smem_inv;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = p.csize;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e;
+    switch (p.vpt) {
+        case 1: e = cudaLaunchKernelEx(&cfg, k_inv_plane<1>, q, b1, sens, eph_l, g, first, tw, done, err); break;
+        case 2: e = cudaLaunchKernelEx(&cfg, k_inv_plane<2>, q, b1, sens, eph_l, g, first, tw, done, err); break;
+        case 4: e = cudaLaunchKernelEx(&cfg, k_inv_plane<4>, q, b1, sens, eph_l, g, first, tw, done, err); break;
+        case 8: e = cudaLaunchKernelEx(&cfg, k_inv_plane<8>, q, b1, sens, eph_l, g, first, tw, done, err); break;
+        case 16: e = cudaLaunchKernelEx(&cfg, k_inv_plane<16>, q, b1, sens, eph_l, g, first, tw, done, err); break;
+        case 32: e = cudaLaunchKernelEx(&cfg, k_inv_plane<32>, q, b1, sens, eph_l, g, first, tw, done, err); break;
+        default: return cudaErrorInvalidValue;
+    }
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+}  // namespace imp

@@ -30,6 +30,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstddef>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -530,10 +531,12 @@ void ToepSolver::release() {
     std::memset(planq_dims_, 0, sizeof(planq_dims_));
     std::memset(planf_dims_, 0, sizeof(planf_dims_));
     void *bufs[] = {sens_, eph_, fm_, qf_, pad_, big_, x_, r_, p_, q_, best_, fhd_, w_, dots_,
-                    t_, grid_};
+                    t_, grid_, qf2_, b1_, tw_};
     for (void *b : bufs)
         if (b) cudaFree(b);
     sens_ = eph_ = qf_ = pad_ = big_ = x_ = r_ = p_ = q_ = best_ = fhd_ = grid_ = nullptr;
+    qf2_ = b1_ = tw_ = nullptr;
+    fast_ = false;
     fm_ = w_ = t_ = nullptr;
     dots_ = nullptr;
     grid_cells_ = 0;
@@ -604,25 +607,39 @@ cudaError_t ToepSolver::setup(const ToepConfig &cfg, const float *t, const float
     T_TRY(cudaMemcpyAsync(t_, t, sizeof(float) * cfg.M, cudaMemcpyDeviceToDevice, st));
     T_TRY(cudaMalloc(&sens_, sizeof(float2) * C * N_));
     T_TRY(cudaMalloc(&eph_, sizeof(float2) * L1 * N_));
-    T_TRY(cudaMalloc(&qf_, sizeof(float2) * L1 * G2_));
-    T_TRY(cudaMalloc(&pad_, sizeof(float2) * C * G2_));
-    T_TRY(cudaMalloc(&big_, sizeof(float2) * C * G2_));
+    // The pruned FFT engine needs power-of-two image sizes; other sizes (and
+    // IMP_TOEP_CUFFT=1) use the zero-padded cuFFT chain.
+    const char *force_cufft = std::getenv("IMP_TOEP_CUFFT");
+    fast_ = !(force_cufft && force_cufft[0] == '1') &&
+            toep_fft_plan(nv[0], is3d ? nv[1] : 1, is3d ? nv[2] : nv[1], C, &fp_);
+    if (fast_) {
+        T_TRY(cudaMalloc(&qf_, sizeof(float2) * G2_));  // one segment, before permutation
+        T_TRY(cudaMalloc(&qf2_, sizeof(float2) * L1 * G2_));
+        T_TRY(cudaMalloc(&b1_, sizeof(float2) * fp_.b1_elems()));
+        T_TRY(toep_fft_twiddles(&tw_));
+    } else {
+        T_TRY(cudaMalloc(&qf_, sizeof(float2) * L1 * G2_));
+        T_TRY(cudaMalloc(&pad_, sizeof(float2) * C * G2_));
+        T_TRY(cudaMalloc(&big_, sizeof(float2) * C * G2_));
+    }
     for (float2 **b : {&x_, &r_, &p_, &q_, &best_, &fhd_}) T_TRY(cudaMalloc(b, sizeof(float2) * N_));
     T_TRY(cudaMalloc(&w_, sizeof(float) * N_));
     T_TRY(cudaMalloc(&dots_, sizeof(double) * (T_SCAL * kTBlocks + 8)));
     T_TRY(cudaMemsetAsync(dots_, 0, sizeof(double) * (T_SCAL * kTBlocks + 8), st));
-    T_TRY(cudaMemsetAsync(pad_, 0, sizeof(float2) * C * G2_, st));
+    if (!fast_) T_TRY(cudaMemsetAsync(pad_, 0, sizeof(float2) * C * G2_, st));
     k_pack_sens_c<<<gridn((size_t)C * N_), kVB, 0, st>>>(sens_, sensi_r, sensi_i, (size_t)C * N_);
     k_eph<<<gridn((size_t)L1 * N_), kVB, 0, st>>>(eph_, fm, N_, L1, tau_, t0_);
     T_TRY(cudaGetLastError());
     // batched C2C on the 2N grid (one transform per coil) and a single one for Qf
     int dims[3] = {n2[0], n2[1], n2[2]};
     const int rank = is3d ? 3 : 2;
-    T_FFT(cufftPlanMany(&plan2_, rank, dims, nullptr, 1, (int)G2_, nullptr, 1, (int)G2_, CUFFT_C2C,
-                        C));
+    if (!fast_) {
+        T_FFT(cufftPlanMany(&plan2_, rank, dims, nullptr, 1, (int)G2_, nullptr, 1, (int)G2_,
+                            CUFFT_C2C, C));
+        T_FFT(cufftSetStream(plan2_, st));
+    }
     T_FFT(cufftPlanMany(&plan1_, rank, dims, nullptr, 1, (int)G2_, nullptr, 1, (int)G2_, CUFFT_C2C,
                         1));
-    T_FFT(cufftSetStream(plan2_, st));
     T_FFT(cufftSetStream(plan1_, st));
     launches_ = 2;
     return cudaSuccess;
@@ -658,13 +675,17 @@ cudaError_t ToepSolver::compute_q(const float *kx, const float *ky, const float 
                                                       cfg_.M, g, tau_, t0_, l);
         T_TRY(cudaGetLastError());
         T_FFT(cufftExecC2C(planq_, grid_, grid_, CUFFT_INVERSE));
-        float2 *qf_l = qf_ + (size_t)l * G2_;
+        float2 *qf_l = fast_ ? qf_ : qf_ + (size_t)l * G2_;
         k_q_post<<<gridn(G2_), kVB, 0, st_>>>(grid_, g, n2d, qf_l,
                                              q_out_r ? q_out_r + (size_t)l * G2_ : nullptr,
                                              q_out_i ? q_out_i + (size_t)l * G2_ : nullptr, G2_);
         T_TRY(cudaGetLastError());
         T_FFT(cufftExecC2C(plan1_, qf_l, qf_l, CUFFT_FORWARD));
         launches_ += 2;  // own kernels only (cuFFT launches are not counted)
+        if (fast_) {
+            T_TRY(toep_fft_qf(fp_, qf2_ + (size_t)l * G2_, qf_l, 1.0f / (float)G2_, st_));
+            ++launches_;
+        }
     }
     return cudaStreamSynchronize(st_);
 }
@@ -672,12 +693,16 @@ cudaError_t ToepSolver::compute_q(const float *kx, const float *ky, const float 
 cudaError_t ToepSolver::load_q(const float *q_r, const float *q_i) {
     const NV n2d{{n2[0], n2[1], n2[2]}};
     for (int l = 0; l <= L_; ++l) {
-        float2 *qf_l = qf_ + (size_t)l * G2_;
+        float2 *qf_l = fast_ ? qf_ : qf_ + (size_t)l * G2_;
         k_q_shift<<<gridn(G2_), kVB, 0, st_>>>(q_r + (size_t)l * G2_, q_i + (size_t)l * G2_, n2d,
                                               cfg_.nz > 1, qf_l, G2_);
         T_TRY(cudaGetLastError());
         T_FFT(cufftExecC2C(plan1_, qf_l, qf_l, CUFFT_FORWARD));
         launches_ += 1;
+        if (fast_) {
+            T_TRY(toep_fft_qf(fp_, qf2_ + (size_t)l * G2_, qf_l, 1.0f / (float)G2_, st_));
+            ++launches_;
+        }
     }
     return cudaStreamSynchronize(st_);
 }
@@ -720,6 +745,15 @@ cudaError_t ToepSolver::apply_aha(const float2 *p, float2 *q) {
     const int C = cfg_.C;
     const float scale = 1.0f / (float)G2_;
     const double *dots = dots_;
+    if (fast_) {
+        const int *done = reinterpret_cast<const int *>(
+            reinterpret_cast<const char *>(dots_ + T_SCAL * kTBlocks) + offsetof(TScal, done));
+        for (int l = 0; l <= L_; ++l)
+            T_TRY(toep_fft_apply_l(fp_, q, p, sens_, eph_ + (size_t)l * N_, b1_,
+                                   qf2_ + (size_t)l * G2_, l == 0 ? 1 : 0, done, tw_, err_,
+                                   st_));
+        return cudaSuccess;
+    }
     for (int l = 0; l <= L_; ++l) {
         const float2 *eph_l = eph_ + (size_t)l * N_;
         k_pad<<<gridn(N_), kVB, 0, st_>>>(pad_, p, sens_, eph_l, nvv, is3d, N_, G2_, C, dots);

@@ -7,6 +7,8 @@
 #include <cufft.h>
 #include <vector>
 
+#include "toep_fft.cuh"
+
 namespace imp {
 
 // One gridding problem: image size and grid size in gridding axis order
@@ -89,7 +91,7 @@ private:
     float2 *sens_ = nullptr;   // [C][N]
     float2 *eph_ = nullptr;    // [(L+1)][N] exp(-i fm (tau l + t0))
     float *fm_ = nullptr;      // [N]
-    float2 *qf_ = nullptr;     // [(L+1)][G2]
+    float2 *qf_ = nullptr;     // [(L+1)][G2] (one segment of scratch with the engine)
     float2 *pad_ = nullptr;    // [C][G2] zero outside the image block
     float2 *big_ = nullptr;    // [C][G2]
     float2 *x_ = nullptr, *r_ = nullptr, *p_ = nullptr, *q_ = nullptr, *best_ = nullptr;
@@ -105,6 +107,12 @@ private:
     size_t grid_cells_ = 0;
     cudaGraphExec_t g_iter_ = nullptr;
     long launches_ = 0;
+    // pruned FFT engine (power-of-two sizes); the cuFFT chain otherwise
+    bool fast_ = false;
+    ToepFftPlan fp_;
+    float2 *qf2_ = nullptr;    // [(L+1)][G2] Qf_l in parity-major order, scaled 1/G2
+    float2 *b1_ = nullptr;     // [C][half spectrum] engine scratch
+    float2 *tw_ = nullptr;     // twiddle table
 };
 
 }  // namespace imp

@@ -163,6 +163,34 @@ def test_apply_2d_matches_oracle(pkg, ctx):
     assert rel(got, want) < TOL_OP
 
 
+@pytest.mark.parametrize("dims,C,L", [((32, 64, 16), 2, 2), ((128, 64, 1), 3, 1),
+                                      ((8, 4, 2), 1, 0), ((24, 40, 1), 2, 2),
+                                      ((12, 8, 6), 2, 1)])
+def test_apply_sizes_match_oracle(pkg, ctx, dims, C, L):
+    """One A^H A (+ lambda D^H D) application with random Q, field map and
+    sensitivities.  Power-of-two sizes run the pruned FFT engine (one- and
+    two-pass line transforms, 2-D and 3-D); other even sizes run the
+    zero-padded cuFFT chain."""
+    rng = np.random.default_rng(sum(dims) + 7 * C + L)
+    nx, ny, nz = dims
+    N, M, G = nx * ny * nz, 64, grid_elems(dims)
+    c = dict(dims=dims, L=L, cg=1, fdp=1e-2, tv_num=0, os_q=2.0, os_fh=1.5,
+             t=np.sort(rng.uniform(0.0, 0.01, M)).astype(np.float32),
+             kx=np.zeros(M, np.float32),
+             fm=rng.uniform(-300.0, 300.0, N).astype(np.float32),
+             sens=(rng.standard_normal((C, N)) + 1j * rng.standard_normal((C, N))).astype(
+                 np.complex64))
+    if C == 1:  # one coil: unit sensitivities (toeplitz/computeFH.cmem.cu:305-310)
+        c["sens"] = np.ones((1, N), np.complex64)
+    Q = (rng.standard_normal((L + 1, G)) + 1j * rng.standard_normal((L + 1, G))).astype(
+        np.complex64)
+    p = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    got = gpu_apply(pkg, ctx, opts_of(pkg, c), c, Q, p)
+    err = rel(got, oracle_apply(c, Q, p, c["fdp"]))
+    print(f"apply {dims} C={C} L={L}: {err:.2e}")
+    assert err < TOL_OP
+
+
 def test_device_and_host_pointers_agree(pkg, ctx):
     c = load("toep_2d_tv")
     o = opts_of(pkg, c)
