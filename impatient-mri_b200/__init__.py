@@ -42,7 +42,9 @@ EXPORTED = [
     "imp_bf_options_default", "imp_bruteforce_recon", "imp_bruteforce_dir",
     "imp_dataset_info", "imp_mrisolver_main", "imp_measure_alu_peaks",
     "imp_toeplitz_options_default", "imp_toeplitz_q", "imp_toeplitz_fhd", "imp_toeplitz_recon",
-    "imp_toeplitz_apply", "imp_toeplitz_dir",
+    "imp_toeplitz_apply", "imp_toeplitz_dir", "imp_toeplitz_cg",
+    "imp_unet_create", "imp_unet_destroy", "imp_unet_num_params", "imp_unet_get_params",
+    "imp_unet_set_params", "imp_unet_forward", "imp_unet_gradients", "imp_unet_train_step",
 ]
 
 
@@ -115,6 +117,18 @@ def lib() -> ctypes.CDLL:
         L.imp_toeplitz_recon.argtypes = [vp, TO] + [vp] * 7 + [ip] + [vp] * 3 + [ip] * 4
         L.imp_toeplitz_apply.argtypes = [vp, TO] + [vp] * 7 + [ip] + [vp] * 3 + [ip] * 4
         L.imp_toeplitz_dir.argtypes = [ctypes.c_char_p, TO, ip, ip, ip, ctypes.c_char_p, ip]
+        L.imp_toeplitz_cg.argtypes = ([vp, TO] + [vp] * 7 + [ip] + [vp] * 3 + [ip] * 4
+                                      + [ctypes.c_double, ip, ctypes.POINTER(ip)])
+        L.imp_unet_create.argtypes = [vp, ip, ip, ip, ctypes.c_ulonglong, ctypes.POINTER(vp)]
+        L.imp_unet_destroy.argtypes = [vp]
+        L.imp_unet_destroy.restype = None
+        L.imp_unet_num_params.argtypes = [vp]
+        L.imp_unet_num_params.restype = ctypes.c_long
+        L.imp_unet_get_params.argtypes = [vp, vp]
+        L.imp_unet_set_params.argtypes = [vp, vp]
+        L.imp_unet_forward.argtypes = [vp, vp, vp]
+        L.imp_unet_gradients.argtypes = [vp, vp, vp, vp, ctypes.POINTER(fp)]
+        L.imp_unet_train_step.argtypes = [vp, vp, vp, fp, ctypes.POINTER(fp)]
         _lib = L
     return _lib
 
@@ -313,6 +327,68 @@ def toeplitz(idir: str, opts: ToepOptions, direct=False, gpu_id=0, reuseQ=False,
     _check(lib().imp_toeplitz_dir(os.fsencode(idir), ctypes.byref(opts), int(direct), gpu_id,
                                   int(reuseQ), os.fsencode(Qdir) if Qdir else None,
                                   int(writeQ)))
+
+
+def toeplitz_cg(ctx, opts: ToepOptions, x_r, x_i, fhd_r, fhd_i, q_r, q_i, t, num_k, fm,
+                sensi_r, sensi_i, num_coil, nx, ny, nz=1, tol=1e-4, max_iter=100) -> int:
+    """CG from the image in x_r/x_i (overwritten with the result) to relative
+    residual tol; returns the number of CG updates."""
+    it = ctypes.c_int(0)
+    _check(lib().imp_toeplitz_cg(
+        ctx.handle, ctypes.byref(opts), *map(_ptr, (x_r, x_i, fhd_r, fhd_i, q_r, q_i, t)),
+        num_k, _ptr(fm), _ptr(sensi_r), _ptr(sensi_i), num_coil, nx, ny, nz,
+        float(tol), int(max_iter), ctypes.byref(it)))
+    return it.value
+
+
+class UNet:
+    """The BF16 U-Net of the learned warm start (images [batch][2][H*W] float32)."""
+
+    def __init__(self, ctx, batch: int, height: int, width: int, seed: int = 0):
+        self._h = ctypes.c_void_p()
+        self.ctx = ctx
+        _check(lib().imp_unet_create(ctx.handle, batch, height, width, seed,
+                                     ctypes.byref(self._h)))
+        self.batch, self.height, self.width = batch, height, width
+
+    def num_params(self) -> int:
+        return int(lib().imp_unet_num_params(self._h))
+
+    def get_params(self, out=None):
+        out = np.zeros(self.num_params(), np.float32) if out is None else out
+        _check(lib().imp_unet_get_params(self._h, _ptr(out)))
+        return out
+
+    def set_params(self, p):
+        _check(lib().imp_unet_set_params(self._h, _ptr(p)))
+
+    def forward(self, x, y):
+        _check(lib().imp_unet_forward(self._h, _ptr(x), _ptr(y)))
+        return y
+
+    def gradients(self, x, target, grads=None):
+        grads = np.zeros(self.num_params(), np.float32) if grads is None else grads
+        loss = ctypes.c_float()
+        _check(lib().imp_unet_gradients(self._h, _ptr(x), _ptr(target), _ptr(grads),
+                                        ctypes.byref(loss)))
+        return float(loss.value), grads
+
+    def train_step(self, x, target, lr: float) -> float:
+        loss = ctypes.c_float()
+        _check(lib().imp_unet_train_step(self._h, _ptr(x), _ptr(target), float(lr),
+                                         ctypes.byref(loss)))
+        return float(loss.value)
+
+    def close(self):
+        if self._h:
+            lib().imp_unet_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def mriSolver(*args: str) -> int:

@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
     const int lw = __ffs(W) - 1;
     const int w = threadIdx.x & (W - 1), j1 = threadIdx.x >> lw;
     const size_t per_coil = (size_t)NS * ncol;
-    for (int c = 0; c < C; ++c) {
+    for (int c = blockIdx.y; c < C; c += gridDim.y) {  // coils split over blockIdx.y
         float2 *bc = b1 + (size_t)c * per_coil + col0;
         for (int a = 0; a < 2; ++a) {
             {
@@ -661,7 +661,8 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
     }
 #undef IMP_PLANE_CASE
     const int r1 = split_r1(p.ns);
-    const int blocks = p.ncol / p.W;
+    const int cols = p.ncol / p.W;
+    const dim3 blocks(cols, std::max(1, std::min(p.C, (2 * 148 + cols - 1) / cols)));
     const int threads = p.W * r1;
 #define IMP_SLOW_CASE(NSV)                                                                 \
     case NSV:                                                                              \

@@ -55,6 +55,9 @@ struct TScal {
     double norm_fhd;
     int cur;
     int done;
+    double tol;   // stop when sqrt(|r|^2 / |F^H d|^2) < tol
+    int iters;    // CG updates performed since the solve started
+    int pad;
 };
 
 __device__ __forceinline__ TScal *scal(double *dots) {
@@ -402,13 +405,20 @@ __global__ void __launch_bounds__(kVB) k_t_dir(float2 *p, const float2 *r, const
     if (blockIdx.x == 0 && threadIdx.x == 0) S->beta2[S->cur ^ 1] = bnew;
 }
 
-__global__ void k_t_finish(double *dots, double tol) {
+__global__ void k_t_finish(double *dots) {
     TScal *S = scal(dots);
     if (S->done) return;
     const double bnew = S->beta2[S->cur ^ 1];
     if (bnew < S->res_best) S->res_best = bnew;
     S->cur ^= 1;
-    if (sqrt(bnew / S->norm_fhd) < tol) S->done = 1;
+    S->iters += 1;
+    if (sqrt(bnew / S->norm_fhd) < S->tol) S->done = 1;
+}
+
+__global__ void k_t_setup(double *dots, double tol) {
+    TScal *S = scal(dots);
+    S->tol = tol;
+    S->iters = 0;
 }
 
 // TV-pass start: r = fhd - q; p = r; partial |r|^2
@@ -776,7 +786,7 @@ cudaError_t ToepSolver::cg_iteration() {
                                         dots_);
     k_t_update<<<kTBlocks, kVB, 0, st_>>>(x_, r_, p_, q_, (int)N_, dots_);
     k_t_dir<<<kTBlocks, kVB, 0, st_>>>(p_, r_, x_, best_, (int)N_, dots_);
-    k_t_finish<<<1, 1, 0, st_>>>(dots_, 1.0e-16);
+    k_t_finish<<<1, 1, 0, st_>>>(dots_);
     return cudaGetLastError();
 }
 
@@ -808,8 +818,9 @@ cudaError_t ToepSolver::solve(const float *fhd_r, const float *fhd_i, float *x_r
     k_fillf<<<gridn(N_), kVB, 0, st_>>>(w_, 1.f, N_);
     k_t_norm<<<kTBlocks, kVB, 0, st_>>>(fhd_, N, dots_);
     k_t_norm_finish<<<1, kVB, 0, st_>>>(dots_);
+    k_t_setup<<<1, 1, 0, st_>>>(dots_, 1.0e-16);  // recon.cu:2112
     T_TRY(cudaGetLastError());
-    launches_ += 4;
+    launches_ += 5;
     const int iter_launches = 3 * (L_ + 1) + 4;  // own kernels of one CG iteration
     if (cfg_.use_graphs && !g_iter_) T_TRY(capture_graph(st_, &g_iter_, &ToepSolver::cg_iteration, this));
     for (int tv_i = 0; tv_i < std::max(cfg_.tv ? cfg_.tv_num : 1, 1); ++tv_i) {
@@ -841,6 +852,59 @@ cudaError_t ToepSolver::solve(const float *fhd_r, const float *fhd_i, float *x_r
     T_TRY(cudaGetLastError());
     ++launches_;
     return cudaSuccess;
+}
+
+cudaError_t ToepSolver::solve_from(const float *fhd_r, const float *fhd_i, float *x_r,
+                                   float *x_i, double tol, int max_iter, int *iters) {
+    const Grid3 gd{nv[0], nv[1], nv[2]};
+    const int N = (int)N_;
+    if (fhd_r) k_soa2c<<<gridn(N_), kVB, 0, st_>>>(fhd_, fhd_r, fhd_i, N_);
+    k_soa2c<<<gridn(N_), kVB, 0, st_>>>(x_, x_r, x_i, N_);
+    T_TRY(cudaMemcpyAsync(best_, x_, sizeof(float2) * N_, cudaMemcpyDeviceToDevice, st_));
+    k_fillf<<<gridn(N_), kVB, 0, st_>>>(w_, 1.f, N_);
+    k_t_norm<<<kTBlocks, kVB, 0, st_>>>(fhd_, N, dots_);
+    k_t_norm_finish<<<1, kVB, 0, st_>>>(dots_);
+    k_t_setup<<<1, 1, 0, st_>>>(dots_, tol);
+    T_TRY(cudaGetLastError());
+    launches_ += 6;
+    if (cfg_.use_graphs && !g_iter_) T_TRY(capture_graph(st_, &g_iter_, &ToepSolver::cg_iteration, this));
+    // The kernels return at once while `done` is set (a previous solve may have
+    // stopped on its tolerance): clear it before the first A^H A.
+    T_TRY(cudaMemsetAsync(reinterpret_cast<char *>(dots_ + T_SCAL * kTBlocks) +
+                              offsetof(TScal, done),
+                          0, sizeof(int), st_));
+    // r = F^H d - A x0; p = r
+    T_TRY(apply_aha(x_, q_));
+    k_t_tvdot<<<kTBlocks, kVB, 0, st_>>>(q_, x_, w_, N, gd, cfg_.fd ? 1 : 0, cfg_.lambda, dots_);
+    k_t_init<<<kTBlocks, kVB, 0, st_>>>(r_, p_, fhd_, q_, N, dots_);
+    k_t_init_finish<<<1, kVB, 0, st_>>>(dots_);
+    T_TRY(cudaGetLastError());
+    launches_ += 3 * (L_ + 1) + 3;
+    const int iter_launches = 3 * (L_ + 1) + 4;
+    const TScal *S = reinterpret_cast<const TScal *>(dots_ + T_SCAL * kTBlocks);
+    int it = 0;
+    while (it < max_iter) {
+        const int chunk = std::min(4, max_iter - it);
+        for (int k = 0; k < chunk; ++k) {
+            if (g_iter_)
+                T_TRY(cudaGraphLaunch(g_iter_, st_));
+            else
+                T_TRY(cg_iteration());
+            launches_ += iter_launches;
+        }
+        it += chunk;
+        int done = 0;
+        T_TRY(cudaMemcpyAsync(&done, &S->done, sizeof(int), cudaMemcpyDeviceToHost, st_));
+        T_TRY(cudaStreamSynchronize(st_));
+        if (done) break;
+    }
+    if (iters) {
+        T_TRY(cudaMemcpyAsync(iters, &S->iters, sizeof(int), cudaMemcpyDeviceToHost, st_));
+        T_TRY(cudaStreamSynchronize(st_));
+    }
+    k_c2soa<<<gridn(N_), kVB, 0, st_>>>(x_r, x_i, best_, N_);
+    ++launches_;
+    return cudaGetLastError();
 }
 
 cudaError_t ToepSolver::apply(const float *p_r, const float *p_i, float *q_r, float *q_i) {
@@ -1055,6 +1119,43 @@ imp_status imp_toeplitz_recon(imp_context *ctx, const imp_toeplitz_options *opt,
         (s = imp::out_device(ctx, x_i, N, keep, &dxi, &hi)))
         return s;
     IMP_CUDA(ts->solve(dfr, dfi, dxr, dxi), "toeplitz CG");
+    if (hr && (s = copy_out(ctx, x_r, dxr, N))) return s;
+    if (hi && (s = copy_out(ctx, x_i, dxi, N))) return s;
+    s = imp::finish(ctx);
+    ctx->launches = ts->launches();
+    return s;
+}
+
+imp_status imp_toeplitz_cg(imp_context *ctx, const imp_toeplitz_options *opt, float *x_r,
+                           float *x_i, const float *fhd_r, const float *fhd_i, const float *q_r,
+                           const float *q_i, const float *t, int num_k, const float *fm,
+                           const float *sensi_r, const float *sensi_i, int num_coil, int nx,
+                           int ny, int nz, double tol, int max_iter, int *iterations) {
+    if (!x_r || !x_i || !fhd_r || !fhd_i) return fail(IMP_ERR_INVALID_ARG, "null array argument");
+    if (max_iter < 0 || !(tol >= 0.0)) return fail(IMP_ERR_INVALID_ARG, "max_iter >= 0, tol >= 0");
+    imp_toeplitz_options o = *opt;
+    o.enable_tv = 0;  // one CG run, no reweighting passes
+    DevKeep keep;
+    imp::ToepSolver *ts = nullptr;
+    imp_status s = toeplitz_common(ctx, &o, q_r, q_i, t, num_k, fm, sensi_r, sensi_i, num_coil,
+                                   nx, ny, nz, keep, &ts);
+    if (s != IMP_OK) return s;
+    const size_t N = (size_t)nx * ny * nz;
+    const float *dfr, *dfi, *dx0r, *dx0i;
+    float *dxr, *dxi;
+    bool hr, hi;
+    if ((s = imp::to_device(ctx, fhd_r, N, keep, &dfr, nullptr)) ||
+        (s = imp::to_device(ctx, fhd_i, N, keep, &dfi, nullptr)) ||
+        (s = imp::to_device(ctx, x_r, N, keep, &dx0r, nullptr)) ||
+        (s = imp::to_device(ctx, x_i, N, keep, &dx0i, nullptr)) ||
+        (s = imp::out_device(ctx, x_r, N, keep, &dxr, &hr)) ||
+        (s = imp::out_device(ctx, x_i, N, keep, &dxi, &hi)))
+        return s;
+    if (hr) IMP_CUDA(cudaMemcpyAsync(dxr, dx0r, N * 4, cudaMemcpyDeviceToDevice, ctx->stream), "x0");
+    if (hi) IMP_CUDA(cudaMemcpyAsync(dxi, dx0i, N * 4, cudaMemcpyDeviceToDevice, ctx->stream), "x0");
+    int it = 0;
+    IMP_CUDA(ts->solve_from(dfr, dfi, dxr, dxi, tol, max_iter, &it), "toeplitz warm CG");
+    if (iterations) *iterations = it;
     if (hr && (s = copy_out(ctx, x_r, dxr, N))) return s;
     if (hi && (s = copy_out(ctx, x_i, dxi, N))) return s;
     s = imp::finish(ctx);

@@ -65,6 +65,10 @@ public:
                             const float *kd_r, const float *kd_i, float *fhd_r, float *fhd_i);
     // Toeplitz CG from x = 0; fhd (device SoA [N]); result = best-residual iterate.
     cudaError_t solve(const float *fhd_r, const float *fhd_i, float *x_r, float *x_i);
+    // CG from x (device SoA, in: x0, out: minimum-residual iterate) until
+    // sqrt(|r|^2/|F^H d|^2) < tol or max_iter updates; no TV passes.
+    cudaError_t solve_from(const float *fhd_r, const float *fhd_i, float *x_r, float *x_i,
+                           double tol, int max_iter, int *iters);
     // One application of A^H A (+ lambda D^H W D with W = 1) for tests.
     cudaError_t apply(const float *p_r, const float *p_i, float *q_r, float *q_i);
 

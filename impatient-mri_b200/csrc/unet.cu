@@ -1,0 +1,907 @@
+// BF16 U-Net for the learned CG warm start (see unet.cuh).
+//
+// Convolutions are implicit GEMMs on the tensor cores (BF16 operands, FP32
+// accumulation): forward and data-gradient share one kernel (the data
+// gradient is the forward conv of the masked output gradient with flipped,
+// transposed weights); the weight gradient is a split-K GEMM over pixels.
+// Tiles are staged with cp.async double buffering.
+#include "common.cuh"
+#include "unet.cuh"
+
+#include <mma.h>
+
+#include <algorithm>
+#include <cmath>
+#include <random>
+#include <vector>
+
+namespace imp {
+
+using bf16 = __nv_bfloat16;
+using namespace nvcuda;
+
+namespace {
+
+constexpr int kCT = 128;  // threads of the GEMM kernels (4 warps, 2 x 2)
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
+    const unsigned s = smem_u32(smem);
+    const int sz = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(sz)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+struct ConvArgs {
+    const bf16 *x;
+    int ldx, xoff;          // input channel stride and offset
+    const bf16 *w;          // [cout][ks*ks*cin]
+    const float *bias;      // [cout] or null
+    bf16 *y;                // BF16 output or null
+    int ldy, yoff;
+    float *yf;              // FP32 output or null
+    int ldyf, yfoff, accumulate;
+    int B, H, W, cin, cout, ks, relu;
+};
+
+// out[p][co] = act(bias + sum_{tap, ci} in[p + shift(tap)][ci] w[co][tap][ci]),
+// zero padding; 64 pixels x 64 output channels per block.
+template <int BK>
+__global__ void __launch_bounds__(kCT) k_conv_fwd(ConvArgs a) {
+    constexpr int LDA = BK + 8;
+    constexpr int STAGE = 64 * LDA;
+    constexpr int SMEM_AB = 2 * 2 * STAGE * (int)sizeof(bf16);
+    constexpr int SMEM_C = 64 * 68 * (int)sizeof(float);
+    __shared__ __align__(128) unsigned char sraw[SMEM_AB > SMEM_C ? SMEM_AB : SMEM_C];
+    bf16 *As = reinterpret_cast<bf16 *>(sraw);
+    bf16 *Bs = As + 2 * STAGE;
+    const int P = a.B * a.H * a.W;
+    const int m0 = blockIdx.x * 64, n0 = blockIdx.y * 64;
+    const int K = a.ks * a.ks * a.cin;
+    const int nk = K / BK;
+    const int half = a.ks / 2;
+    auto load = [&](int kt, int stage) {
+        const int k0 = kt * BK;
+        const int tap = k0 / a.cin, c0 = k0 % a.cin;
+        const int dy = tap / a.ks - half, dx = tap % a.ks - half;
+        constexpr int CPR = BK / 8;
+        for (int id = threadIdx.x; id < 64 * CPR; id += kCT) {
+            const int m = id / CPR, j = id % CPR;
+            const int p = m0 + m;
+            bool valid = p < P;
+            const bf16 *src = a.x;
+            if (valid) {
+                const int xx = p % a.W, yy = (p / a.W) % a.H;
+                const int ys = yy + dy, xs = xx + dx;
+                valid = ys >= 0 && ys < a.H && xs >= 0 && xs < a.W;
+                if (valid)
+                    src = a.x + (size_t)(p + dy * a.W + dx) * a.ldx + a.xoff + c0 + j * 8;
+            }
+            cp_async16(As + stage * STAGE + m * LDA + j * 8, src, valid);
+        }
+        for (int id = threadIdx.x; id < 64 * CPR; id += kCT) {
+            const int n = id / CPR, j = id % CPR;
+            const int co = n0 + n;
+            const bool valid = co < a.cout;
+            const bf16 *src = valid ? a.w + (size_t)co * K + k0 + j * 8 : a.w;
+            cp_async16(Bs + stage * STAGE + n * LDA + j * 8, src, valid);
+        }
+        cp_async_commit();
+    };
+    const int warp = threadIdx.x >> 5, wm = warp >> 1, wn = warp & 1;
+    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[2][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) wmma::fill_fragment(acc[i][j], 0.f);
+    load(0, 0);
+    for (int kt = 0; kt < nk; ++kt) {
+        if (kt + 1 < nk) {
+            load(kt + 1, (kt + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const bf16 *as = As + (kt & 1) * STAGE;
+        const bf16 *bs = Bs + (kt & 1) * STAGE;
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk) {
+            wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::row_major> fa[2];
+            wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::col_major> fb[2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+                wmma::load_matrix_sync(fa[i], as + (wm * 32 + i * 16) * LDA + kk * 16, LDA);
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+                wmma::load_matrix_sync(fb[j], bs + (wn * 32 + j * 16) * LDA + kk * 16, LDA);
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) wmma::mma_sync(acc[i][j], fa[i], fb[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+    float *Cs = reinterpret_cast<float *>(sraw);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+            wmma::store_matrix_sync(Cs + (wm * 32 + i * 16) * 68 + wn * 32 + j * 16, acc[i][j], 68,
+                                    wmma::mem_row_major);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < 64 * 64; idx += kCT) {
+        const int m = idx >> 6, n = idx & 63;
+        const int p = m0 + m, co = n0 + n;
+        if (p >= P || co >= a.cout) continue;
+        float v = Cs[m * 68 + n];
+        if (a.bias) v += a.bias[co];
+        if (a.relu) v = fmaxf(v, 0.f);
+        if (a.y) a.y[(size_t)p * a.ldy + a.yoff + co] = __float2bfloat16(v);
+        if (a.yf) {
+            float *d = a.yf + (size_t)p * a.ldyf + a.yfoff + co;
+            *d = a.accumulate ? *d + v : v;
+        }
+    }
+}
+
+struct WgArgs {
+    const bf16 *dz;   // [P][cout]
+    const bf16 *x;    // input, channel stride ldx, offset xoff
+    int ldx, xoff;
+    float *dw;        // [cout][ks*ks*cin] (accumulated with atomics)
+    int B, H, W, cin, cout, ks, splits;
+};
+
+// dw[co][tap][ci] += sum_p dz[p][co] x[p + shift(tap)][ci]; block = 64 x 64
+// (co, ci) for one tap and one pixel range; 32 pixels per k-step.
+__global__ void __launch_bounds__(kCT) k_wgrad(WgArgs a) {
+    constexpr int LD = 72;
+    constexpr int STAGE = 32 * LD;
+    constexpr int SMEM_AB = 2 * 2 * STAGE * (int)sizeof(bf16);
+    constexpr int SMEM_C = 64 * 68 * (int)sizeof(float);
+    __shared__ __align__(128) unsigned char sraw[SMEM_AB > SMEM_C ? SMEM_AB : SMEM_C];
+    bf16 *As = reinterpret_cast<bf16 *>(sraw);
+    bf16 *Bs = As + 2 * STAGE;
+    const int P = a.B * a.H * a.W;
+    const int taps = a.ks * a.ks;
+    const int tap = blockIdx.z % taps, split = blockIdx.z / taps;
+    const int co0 = blockIdx.x * 64, ci0 = blockIdx.y * 64;
+    const int half = a.ks / 2;
+    const int dy = tap / a.ks - half, dx = tap % a.ks - half;
+    const int chunk = ((P + a.splits - 1) / a.splits + 31) / 32 * 32;
+    const int p0 = split * chunk, p1 = min(P, p0 + chunk);
+    if (p0 >= p1) return;
+    const int nk = (p1 - p0 + 31) / 32;
+    auto load = [&](int kt, int stage) {
+        for (int id = threadIdx.x; id < 32 * 8; id += kCT) {
+            const int r = id >> 3, j = id & 7;
+            const int p = p0 + kt * 32 + r;
+            const bool pv = p < p1;
+            const bool av = pv && co0 + j * 8 < a.cout;
+            cp_async16(As + stage * STAGE + r * LD + j * 8,
+                       av ? a.dz + (size_t)p * a.cout + co0 + j * 8 : a.dz, av);
+            bool bv = pv && ci0 + j * 8 < a.cin;
+            const bf16 *src = a.x;
+            if (bv) {
+                const int xx = p % a.W, yy = (p / a.W) % a.H;
+                const int ys = yy + dy, xs = xx + dx;
+                bv = ys >= 0 && ys < a.H && xs >= 0 && xs < a.W;
+                if (bv) src = a.x + (size_t)(p + dy * a.W + dx) * a.ldx + a.xoff + ci0 + j * 8;
+            }
+            cp_async16(Bs + stage * STAGE + r * LD + j * 8, src, bv);
+        }
+        cp_async_commit();
+    };
+    const int warp = threadIdx.x >> 5, wm = warp >> 1, wn = warp & 1;
+    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[2][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) wmma::fill_fragment(acc[i][j], 0.f);
+    load(0, 0);
+    for (int kt = 0; kt < nk; ++kt) {
+        if (kt + 1 < nk) {
+            load(kt + 1, (kt + 1) & 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const bf16 *as = As + (kt & 1) * STAGE;
+        const bf16 *bs = Bs + (kt & 1) * STAGE;
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {
+            wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, wmma::col_major> fa[2];
+            wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, wmma::row_major> fb[2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+                wmma::load_matrix_sync(fa[i], as + kk * 16 * LD + wm * 32 + i * 16, LD);
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+                wmma::load_matrix_sync(fb[j], bs + kk * 16 * LD + wn * 32 + j * 16, LD);
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) wmma::mma_sync(acc[i][j], fa[i], fb[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+    float *Cs = reinterpret_cast<float *>(sraw);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+            wmma::store_matrix_sync(Cs + (wm * 32 + i * 16) * 68 + wn * 32 + j * 16, acc[i][j], 68,
+                                    wmma::mem_row_major);
+    __syncthreads();
+    const int K = taps * a.cin;
+    for (int idx = threadIdx.x; idx < 64 * 64; idx += kCT) {
+        const int m = idx >> 6, n = idx & 63;
+        const int co = co0 + m, ci = ci0 + n;
+        if (co >= a.cout || ci >= a.cin) continue;
+        atomicAdd(&a.dw[(size_t)co * K + tap * a.cin + ci], Cs[m * 68 + n]);
+    }
+}
+
+// db[co] += sum_p dz[p][co]
+__global__ void k_bgrad(float *db, const bf16 *dz, int P, int cout) {
+    const int pb = blockIdx.x * 256;
+    const int pe = min(P, pb + 256);
+    for (int c = threadIdx.x; c < cout; c += blockDim.x) {
+        float s = 0.f;
+        for (int p = pb; p < pe; ++p) s += __bfloat162float(dz[(size_t)p * cout + c]);
+        atomicAdd(&db[c], s);
+    }
+}
+
+// dz[p][co] = g[p][goff + co] * (relu ? (y[p][yoff + co] > 0) : 1), as BF16
+__global__ void k_dz(bf16 *dz, const float *g, int ldg, int goff, const bf16 *y, int ldy, int yoff,
+                     int P, int cout, int relu) {
+    const size_t n = (size_t)P * cout;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t p = i / cout;
+        const int c = (int)(i % cout);
+        float v = g[p * ldg + goff + c];
+        if (relu && !(__bfloat162float(y[p * ldy + yoff + c]) > 0.f)) v = 0.f;
+        dz[i] = __float2bfloat16(v);
+    }
+}
+
+// wt[ci][taps - 1 - t][co] = w[co][t][ci]
+__global__ void k_wtrans(bf16 *wt, const bf16 *w, int cin, int cout, int taps) {
+    const size_t n = (size_t)cin * cout * taps;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int ci = (int)(i % cin);
+        const size_t r = i / cin;
+        const int t = (int)(r % taps);
+        const int co = (int)(r / taps);
+        wt[((size_t)ci * taps + (taps - 1 - t)) * cout + co] = w[i];
+    }
+}
+
+// 2x2 max pooling; idx = argmax position (dy * 2 + dx)
+__global__ void k_pool_fwd(bf16 *out, unsigned char *idx, const bf16 *in, int ldi, int ioff, int B,
+                           int H, int W, int C) {
+    const int Ho = H / 2, Wo = W / 2;
+    const size_t n = (size_t)B * Ho * Wo * C;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const size_t q = i / C;
+        const int xo = (int)(q % Wo), yo = (int)((q / Wo) % Ho), b = (int)(q / ((size_t)Wo * Ho));
+        float best = -INFINITY;
+        int bi = 0;
+        for (int d = 0; d < 4; ++d) {
+            const size_t p = ((size_t)b * H + 2 * yo + (d >> 1)) * W + 2 * xo + (d & 1);
+            const float v = __bfloat162float(in[p * ldi + ioff + c]);
+            if (v > best) {
+                best = v;
+                bi = d;
+            }
+        }
+        out[i] = __float2bfloat16(best);
+        idx[i] = (unsigned char)bi;
+    }
+}
+
+__global__ void k_pool_bwd(float *gin, int ldg, int goff, const float *gout,
+                           const unsigned char *idx, int B, int H, int W, int C) {
+    const int Ho = H / 2, Wo = W / 2;
+    const size_t n = (size_t)B * Ho * Wo * C;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const size_t q = i / C;
+        const int xo = (int)(q % Wo), yo = (int)((q / Wo) % Ho), b = (int)(q / ((size_t)Wo * Ho));
+        const int d = idx[i];
+        const size_t p = ((size_t)b * H + 2 * yo + (d >> 1)) * W + 2 * xo + (d & 1);
+        gin[p * ldg + goff + c] += gout[i];
+    }
+}
+
+// nearest x2: out[b][y][x][off + c] = in[b][y/2][x/2][c]  (H, W: output size)
+__global__ void k_up_fwd(bf16 *out, int ldo, int ooff, const bf16 *in, int B, int H, int W,
+                         int C) {
+    const size_t n = (size_t)B * H * W * C;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const size_t p = i / C;
+        const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
+        const size_t pi = ((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2;
+        out[p * ldo + ooff + c] = in[pi * C + c];
+    }
+}
+
+// gin[b][i][j][c] = sum of the 2 x 2 block of gout[..][goff + c]  (H, W: input size)
+__global__ void k_up_bwd(float *gin, const float *gout, int ldg, int goff, int B, int H, int W,
+                         int C) {
+    const size_t n = (size_t)B * H * W * C;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i % C);
+        const size_t p = i / C;
+        const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
+        float s = 0.f;
+        for (int d = 0; d < 4; ++d) {
+            const size_t po = ((size_t)b * 2 * H + 2 * y + (d >> 1)) * (2 * W) + 2 * x + (d & 1);
+            s += gout[po * ldg + goff + c];
+        }
+        gin[i] += s;
+    }
+}
+
+// x [B][2][HW] -> X0 [P][16] (channels 2..15 zero)
+__global__ void k_pack(bf16 *x0, const float *x, int B, int HW) {
+    const size_t n = (size_t)B * HW * 16;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(i & 15);
+        const size_t p = i >> 4;
+        const size_t b = p / HW, r = p % HW;
+        x0[i] = __float2bfloat16(c < 2 ? x[(b * 2 + c) * HW + r] : 0.f);
+    }
+}
+
+__global__ void k_unpack(float *y, const float *outf, int B, int HW) {
+    const size_t n = (size_t)B * 2 * HW;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i % HW, bc = i / HW;
+        const size_t b = bc / 2, c = bc % 2;
+        y[i] = outf[(b * HW + r) * 16 + c];
+    }
+}
+
+// gout[p][c] = 2 (out - t) / n for c < 2; per-block partial sums of (out - t)^2
+__global__ void k_loss(float *gout, double *part, const float *outf, const float *t, int B,
+                       int HW) {
+    __shared__ double sh[33];
+    const size_t n = (size_t)B * 2 * HW;
+    const float sc = 2.0f / (float)n;
+    double loc = 0.0;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const size_t r = i % HW, bc = i / HW;
+        const size_t b = bc / 2, c = bc % 2;
+        const size_t o = (b * HW + r) * 16 + c;
+        const float d = outf[o] - t[i];
+        gout[o] = sc * d;
+        loc += (double)d * d;
+    }
+    const double s = block_sum(loc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void k_adam(float *p, float *m, float *v, const float *g, size_t n, float lr,
+                       float b1c, float b2c) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = 0.9f * m[i] + 0.1f * gi;
+        const float vi = 0.999f * v[i] + 0.001f * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / b1c) / (sqrtf(vi / b2c) + 1e-8f);
+    }
+}
+
+__global__ void k_to_bf16(bf16 *o, const float *s, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+         i += (size_t)gridDim.x * blockDim.x)
+        o[i] = __float2bfloat16(s[i]);
+}
+
+int gridn_u(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 32); }
+
+constexpr int kLossBlocks = 296;
+
+}  // namespace
+
+#define U_TRY(x)                              \
+    do {                                      \
+        cudaError_t e_ = (x);                 \
+        if (e_ != cudaSuccess) return e_;     \
+    } while (0)
+
+UNet::~UNet() { release(); }
+
+void UNet::release() {
+    for (void *p : {(void *)master_, (void *)grad_, (void *)m_, (void *)v_, (void *)wb_,
+                    (void *)wt_, (void *)dz_, (void *)pidx_, (void *)scratch_, (void *)outg_})
+        if (p) cudaFree(p);
+    master_ = grad_ = m_ = v_ = outg_ = nullptr;
+    scratch_ = nullptr;
+    wb_ = wt_ = dz_ = nullptr;
+    pidx_ = nullptr;
+    for (Act &a : acts_) {
+        if (a.v) cudaFree(a.v);
+        if (a.g) cudaFree(a.g);
+    }
+    acts_.clear();
+    layers_.clear();
+}
+
+// Activation indices.
+enum {
+    A_X0, A_E1A, A_D1, A_P1, A_E2A, A_D2, A_P2, A_E3A, A_D3, A_P3, A_M1, A_M2, A_T3, A_F3A,
+    A_F3B, A_T2, A_F2A, A_F2B, A_T1, A_F1A, A_F1B, A_OUT, A_COUNT
+};
+
+cudaError_t UNet::setup(int batch, int H, int W, unsigned long long seed, cudaStream_t st) {
+    release();
+    st_ = st;
+    B_ = batch;
+    H_ = H;
+    W_ = W;
+    step_ = 0;
+    const int cfg[18][4] = {  // cin, cout, ks, relu
+        {16, 32, 3, 1},   {32, 32, 3, 1},   {32, 64, 3, 1},   {64, 64, 3, 1},
+        {64, 128, 3, 1},  {128, 128, 3, 1}, {128, 256, 3, 1}, {256, 256, 3, 1},
+        {256, 128, 1, 0}, {256, 128, 3, 1}, {128, 128, 3, 1}, {128, 64, 1, 0},
+        {128, 64, 3, 1},  {64, 64, 3, 1},   {64, 32, 1, 0},   {64, 32, 3, 1},
+        {32, 32, 3, 1},   {32, 16, 1, 0}};
+    size_t off = 0;
+    for (auto &c : cfg) {
+        ConvLayer L;
+        L.cin = c[0];
+        L.cout = c[1];
+        L.ks = c[2];
+        L.relu = c[3] != 0;
+        L.w_off = off;
+        off += L.wsize();
+        L.b_off = off;
+        off += L.cout;
+        layers_.push_back(L);
+    }
+    n_params_ = off;
+    // He initialisation (seeded, host); the zero input channels 2..15 of the
+    // first layer and the unused outputs 2..15 of the last stay zero.
+    std::vector<float> h(n_params_, 0.f);
+    std::mt19937_64 rng(seed);
+    for (size_t li = 0; li < layers_.size(); ++li) {
+        const ConvLayer &L = layers_[li];
+        const int cin_eff = li == 0 ? 2 : L.cin;
+        const double sd = std::sqrt((L.relu ? 2.0 : 1.0) / (L.ks * L.ks * cin_eff));
+        std::normal_distribution<double> nd(0.0, sd);
+        const int taps = L.ks * L.ks;
+        for (int co = 0; co < L.cout; ++co) {
+            if (li + 1 == layers_.size() && co >= 2) continue;
+            for (int t = 0; t < taps; ++t)
+                for (int ci = 0; ci < cin_eff; ++ci)
+                    h[L.w_off + ((size_t)co * taps + t) * L.cin + ci] = (float)nd(rng);
+        }
+    }
+    const size_t pb = n_params_ * sizeof(float);
+    U_TRY(cudaMalloc(&master_, pb));
+    U_TRY(cudaMalloc(&grad_, pb));
+    U_TRY(cudaMalloc(&m_, pb));
+    U_TRY(cudaMalloc(&v_, pb));
+    U_TRY(cudaMalloc(&wb_, n_params_ * sizeof(bf16)));
+    U_TRY(cudaMalloc(&wt_, n_params_ * sizeof(bf16)));
+    U_TRY(cudaMemcpy(master_, h.data(), pb, cudaMemcpyHostToDevice));
+    U_TRY(cudaMemsetAsync(m_, 0, pb, st));
+    U_TRY(cudaMemsetAsync(v_, 0, pb, st));
+    // activations
+    const int Hs[4] = {H, H / 2, H / 4, H / 8}, Ws[4] = {W, W / 2, W / 4, W / 8};
+    const int shape[A_COUNT][2] = {  // level, channels
+        {0, 16}, {0, 32}, {0, 64}, {1, 32}, {1, 64}, {1, 128}, {2, 64}, {2, 128},
+        {2, 256}, {3, 128}, {3, 256}, {3, 256}, {3, 128}, {2, 128}, {2, 128}, {2, 64},
+        {1, 64}, {1, 64}, {1, 32}, {0, 32}, {0, 32}, {0, 16}};
+    acts_.resize(A_COUNT);
+    size_t max_dz = 0;
+    for (int i = 0; i < A_COUNT; ++i) {
+        Act &a = acts_[i];
+        a.H = Hs[shape[i][0]];
+        a.W = Ws[shape[i][0]];
+        a.C = shape[i][1];
+        const size_t n = (size_t)B_ * a.H * a.W * a.C;
+        U_TRY(cudaMalloc(&a.v, n * sizeof(bf16)));
+        U_TRY(cudaMalloc(&a.g, n * sizeof(float)));
+        max_dz = std::max(max_dz, n);
+    }
+    U_TRY(cudaMalloc(&dz_, max_dz * sizeof(bf16)));
+    size_t pidx = 0;
+    const int pool_src[3] = {A_P1, A_P2, A_P3};
+    for (int l = 0; l < 3; ++l) {
+        const Act &a = acts_[pool_src[l]];
+        pidx_off_[l] = pidx;
+        pidx += (size_t)B_ * a.H * a.W * a.C;
+    }
+    U_TRY(cudaMalloc(&pidx_, pidx));
+    U_TRY(cudaMalloc(&scratch_, kLossBlocks * sizeof(double)));
+    U_TRY(cudaMalloc(&outg_, (size_t)B_ * H_ * W_ * 16 * sizeof(float)));
+    return sync_weights();
+}
+
+cudaError_t UNet::sync_weights() {
+    k_to_bf16<<<gridn_u(n_params_), 256, 0, st_>>>(wb_, master_, n_params_);
+    ++launches_;
+    for (const ConvLayer &L : layers_) {
+        k_wtrans<<<gridn_u(L.wsize()), 256, 0, st_>>>(wt_ + L.w_off, wb_ + L.w_off, L.cin, L.cout,
+                                                      L.ks * L.ks);
+        ++launches_;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t UNet::conv_fwd(int li, const Act &in, int in_off, Act &out, int out_off) {
+    const ConvLayer &L = layers_[li];
+    ConvArgs a{};
+    a.x = in.v;
+    a.ldx = in.C;
+    a.xoff = in_off;
+    a.w = wb_ + L.w_off;
+    a.bias = master_ + L.b_off;
+    a.B = B_;
+    a.H = in.H;
+    a.W = in.W;
+    a.cin = L.cin;
+    a.cout = L.cout;
+    a.ks = L.ks;
+    a.relu = L.relu ? 1 : 0;
+    if (&out == &acts_[A_OUT]) {
+        a.yf = out.g;  // the FP32 network output lives in OUT's gradient-sized buffer
+        a.ldyf = out.C;
+        a.yfoff = 0;
+        a.y = nullptr;
+    } else {
+        a.y = out.v;
+        a.ldy = out.C;
+        a.yoff = out_off;
+    }
+    const int P = B_ * in.H * in.W;
+    const dim3 grid((P + 63) / 64, (L.cout + 63) / 64);
+    if (L.cin % 32 == 0)
+        k_conv_fwd<32><<<grid, kCT, 0, st_>>>(a);
+    else
+        k_conv_fwd<16><<<grid, kCT, 0, st_>>>(a);
+    ++launches_;
+    return cudaGetLastError();
+}
+
+// Gradients of layer li whose output is out[..][out_off, +cout) with gradient
+// out.g: weights, bias, and (when in.g is set and li > 0) the input gradient
+// in.g[..][in_off, +cin) += ...
+cudaError_t UNet::conv_bwd(int li, Act &in, int in_off, Act &out, int out_off) {
+    const ConvLayer &L = layers_[li];
+    const int P = B_ * in.H * in.W;
+    const bool is_out = &out == &acts_[A_OUT];
+    k_dz<<<gridn_u((size_t)P * L.cout), 256, 0, st_>>>(
+        dz_, is_out ? outg_ : out.g, out.C, is_out ? 0 : out_off, out.v, out.C,
+        out_off, P, L.cout, L.relu ? 1 : 0);
+    WgArgs w{};
+    w.dz = dz_;
+    w.x = in.v;
+    w.ldx = in.C;
+    w.xoff = in_off;
+    w.dw = grad_ + L.w_off;
+    w.B = B_;
+    w.H = in.H;
+    w.W = in.W;
+    w.cin = L.cin;
+    w.cout = L.cout;
+    w.ks = L.ks;
+    const int base = ((L.cout + 63) / 64) * ((L.cin + 63) / 64) * L.ks * L.ks;
+    w.splits = std::max(1, std::min((P + 31) / 32, 148 * 8 / base));
+    k_wgrad<<<dim3((L.cout + 63) / 64, (L.cin + 63) / 64, L.ks * L.ks * w.splits), kCT, 0, st_>>>(w);
+    k_bgrad<<<(P + 255) / 256, 256, 0, st_>>>(grad_ + L.b_off, dz_, P, L.cout);
+    launches_ += 3;
+    if (li > 0 && in.g) {
+        ConvArgs a{};
+        a.x = dz_;
+        a.ldx = L.cout;
+        a.xoff = 0;
+        a.w = wt_ + L.w_off;
+        a.bias = nullptr;
+        a.y = nullptr;
+        a.yf = in.g;
+        a.ldyf = in.C;
+        a.yfoff = in_off;
+        a.accumulate = 1;
+        a.B = B_;
+        a.H = in.H;
+        a.W = in.W;
+        a.cin = L.cout;
+        a.cout = L.cin;
+        a.ks = L.ks;
+        a.relu = 0;
+        const dim3 grid((P + 63) / 64, (L.cin + 63) / 64);
+        if (L.cout % 32 == 0)
+            k_conv_fwd<32><<<grid, kCT, 0, st_>>>(a);
+        else
+            k_conv_fwd<16><<<grid, kCT, 0, st_>>>(a);
+        ++launches_;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t UNet::pack_input(const float *x) {
+    k_pack<<<gridn_u((size_t)B_ * H_ * W_ * 16), 256, 0, st_>>>(acts_[A_X0].v, x, B_, H_ * W_);
+    ++launches_;
+    return cudaGetLastError();
+}
+
+cudaError_t UNet::run_forward() {
+    auto &A = acts_;
+    auto pool = [&](int src, int lvl, int dst) {
+        const Act &s = A[src];
+        Act &d = A[dst];
+        k_pool_fwd<<<gridn_u((size_t)B_ * d.H * d.W * d.C), 256, 0, st_>>>(
+            d.v, pidx_ + pidx_off_[lvl], s.v, s.C, 0, B_, s.H, s.W, d.C);
+        ++launches_;
+    };
+    auto up = [&](int src, int dst, int off) {
+        const Act &s = A[src];
+        Act &d = A[dst];
+        k_up_fwd<<<gridn_u((size_t)B_ * d.H * d.W * s.C), 256, 0, st_>>>(d.v, d.C, off, s.v, B_,
+                                                                       d.H, d.W, s.C);
+        ++launches_;
+    };
+    U_TRY(conv_fwd(0, A[A_X0], 0, A[A_E1A], 0));
+    U_TRY(conv_fwd(1, A[A_E1A], 0, A[A_D1], 0));
+    pool(A_D1, 0, A_P1);
+    U_TRY(conv_fwd(2, A[A_P1], 0, A[A_E2A], 0));
+    U_TRY(conv_fwd(3, A[A_E2A], 0, A[A_D2], 0));
+    pool(A_D2, 1, A_P2);
+    U_TRY(conv_fwd(4, A[A_P2], 0, A[A_E3A], 0));
+    U_TRY(conv_fwd(5, A[A_E3A], 0, A[A_D3], 0));
+    pool(A_D3, 2, A_P3);
+    U_TRY(conv_fwd(6, A[A_P3], 0, A[A_M1], 0));
+    U_TRY(conv_fwd(7, A[A_M1], 0, A[A_M2], 0));
+    U_TRY(conv_fwd(8, A[A_M2], 0, A[A_T3], 0));
+    up(A_T3, A_D3, 128);
+    U_TRY(conv_fwd(9, A[A_D3], 0, A[A_F3A], 0));
+    U_TRY(conv_fwd(10, A[A_F3A], 0, A[A_F3B], 0));
+    U_TRY(conv_fwd(11, A[A_F3B], 0, A[A_T2], 0));
+    up(A_T2, A_D2, 64);
+    U_TRY(conv_fwd(12, A[A_D2], 0, A[A_F2A], 0));
+    U_TRY(conv_fwd(13, A[A_F2A], 0, A[A_F2B], 0));
+    U_TRY(conv_fwd(14, A[A_F2B], 0, A[A_T1], 0));
+    up(A_T1, A_D1, 32);
+    U_TRY(conv_fwd(15, A[A_D1], 0, A[A_F1A], 0));
+    U_TRY(conv_fwd(16, A[A_F1A], 0, A[A_F1B], 0));
+    U_TRY(conv_fwd(17, A[A_F1B], 0, A[A_OUT], 0));
+    return cudaGetLastError();
+}
+
+cudaError_t UNet::forward(const float *x, float *y) {
+    U_TRY(pack_input(x));
+    U_TRY(run_forward());
+    k_unpack<<<gridn_u((size_t)B_ * 2 * H_ * W_), 256, 0, st_>>>(y, acts_[A_OUT].g, B_, H_ * W_);
+    ++launches_;
+    return cudaGetLastError();
+}
+
+cudaError_t UNet::train_step(const float *x, const float *target, float lr, float *loss) {
+    U_TRY(gradients(x, target, loss));
+    ++step_;
+    const float b1c = 1.0f - std::pow(0.9f, (float)step_);
+    const float b2c = 1.0f - std::pow(0.999f, (float)step_);
+    k_adam<<<gridn_u(n_params_), 256, 0, st_>>>(master_, m_, v_, grad_, n_params_, lr, b1c, b2c);
+    ++launches_;
+    return sync_weights();
+}
+
+cudaError_t UNet::gradients(const float *x, const float *target, float *loss) {
+    auto &A = acts_;
+    U_TRY(pack_input(x));
+    U_TRY(run_forward());
+    // loss and its gradient (the FP32 output sits in OUT.g; its gradient in out_grad)
+    float *og = outg_;
+    U_TRY(cudaMemsetAsync(og, 0, (size_t)B_ * H_ * W_ * 16 * sizeof(float), st_));
+    k_loss<<<kLossBlocks, 256, 0, st_>>>(og, scratch_, A[A_OUT].g, target, B_, H_ * W_);
+    ++launches_;
+    for (int i = 0; i < A_COUNT; ++i)
+        if (i != A_OUT)
+            U_TRY(cudaMemsetAsync(A[i].g, 0, (size_t)B_ * A[i].H * A[i].W * A[i].C * sizeof(float),
+                                  st_));
+    U_TRY(cudaMemsetAsync(grad_, 0, n_params_ * sizeof(float), st_));
+    auto pool_bwd = [&](int dst, int lvl, int src) {  // gradient of pool(dst) -> dst.g
+        Act &d = A[dst];
+        const Act &s = A[src];
+        k_pool_bwd<<<gridn_u((size_t)B_ * s.H * s.W * s.C), 256, 0, st_>>>(
+            d.g, d.C, 0, s.g, pidx_ + pidx_off_[lvl], B_, d.H, d.W, s.C);
+        ++launches_;
+    };
+    auto up_bwd = [&](int src, int dst, int off) {  // d(up(src) -> dst[off]) -> src.g
+        Act &s = A[src];
+        const Act &d = A[dst];
+        k_up_bwd<<<gridn_u((size_t)B_ * s.H * s.W * s.C), 256, 0, st_>>>(s.g, d.g, d.C, off, B_,
+                                                                        s.H, s.W, s.C);
+        ++launches_;
+    };
+    U_TRY(conv_bwd(17, A[A_F1B], 0, A[A_OUT], 0));
+    U_TRY(conv_bwd(16, A[A_F1A], 0, A[A_F1B], 0));
+    U_TRY(conv_bwd(15, A[A_D1], 0, A[A_F1A], 0));
+    up_bwd(A_T1, A_D1, 32);
+    U_TRY(conv_bwd(14, A[A_F2B], 0, A[A_T1], 0));
+    U_TRY(conv_bwd(13, A[A_F2A], 0, A[A_F2B], 0));
+    U_TRY(conv_bwd(12, A[A_D2], 0, A[A_F2A], 0));
+    up_bwd(A_T2, A_D2, 64);
+    U_TRY(conv_bwd(11, A[A_F3B], 0, A[A_T2], 0));
+    U_TRY(conv_bwd(10, A[A_F3A], 0, A[A_F3B], 0));
+    U_TRY(conv_bwd(9, A[A_D3], 0, A[A_F3A], 0));
+    up_bwd(A_T3, A_D3, 128);
+    U_TRY(conv_bwd(8, A[A_M2], 0, A[A_T3], 0));
+    U_TRY(conv_bwd(7, A[A_M1], 0, A[A_M2], 0));
+    U_TRY(conv_bwd(6, A[A_P3], 0, A[A_M1], 0));
+    pool_bwd(A_D3, 2, A_P3);
+    U_TRY(conv_bwd(5, A[A_E3A], 0, A[A_D3], 0));
+    U_TRY(conv_bwd(4, A[A_P2], 0, A[A_E3A], 0));
+    pool_bwd(A_D2, 1, A_P2);
+    U_TRY(conv_bwd(3, A[A_E2A], 0, A[A_D2], 0));
+    U_TRY(conv_bwd(2, A[A_P1], 0, A[A_E2A], 0));
+    pool_bwd(A_D1, 0, A_P1);
+    U_TRY(conv_bwd(1, A[A_E1A], 0, A[A_D1], 0));
+    U_TRY(conv_bwd(0, A[A_X0], 0, A[A_E1A], 0));
+    if (loss) {
+        double part[kLossBlocks];
+        U_TRY(cudaMemcpyAsync(part, scratch_, sizeof(part), cudaMemcpyDeviceToHost, st_));
+        U_TRY(cudaStreamSynchronize(st_));
+        double s = 0.0;
+        for (double p : part) s += p;
+        *loss = (float)(s / ((double)B_ * 2 * H_ * W_));
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace imp
+
+// ============================================================================
+// C-ABI of the learned warm start (no counterpart in the reference)
+// ============================================================================
+#include "context.h"
+
+struct imp_unet {
+    imp_context *ctx = nullptr;
+    imp::UNet net;
+};
+
+using imp::DevKeep;
+using imp::fail;
+
+namespace {
+
+imp_status unet_io(imp_unet *u, const float *x, size_t nx, DevKeep &keep, const float **dx) {
+    return imp::to_device(u->ctx, x, nx, keep, dx, nullptr);
+}
+
+}  // namespace
+
+extern "C" {
+
+imp_status imp_unet_create(imp_context *ctx, int batch, int height, int width,
+                           unsigned long long seed, imp_unet **out) {
+    if (!out) return fail(IMP_ERR_INVALID_ARG, "null output pointer");
+    *out = nullptr;
+    if (batch < 1 || height < 8 || width < 8 || height % 8 || width % 8)
+        return fail(IMP_ERR_INVALID_ARG, "batch >= 1 and height, width multiples of 8 required");
+    imp_status s = imp::begin(ctx);
+    if (s != IMP_OK) return s;
+    imp_unet *u = new imp_unet();
+    u->ctx = ctx;
+    cudaError_t e = u->net.setup(batch, height, width, seed, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        delete u;
+        return imp::from_cuda(e, "unet setup");
+    }
+    *out = u;
+    return IMP_OK;
+}
+
+// Frees the network's device memory (cudaFree synchronizes the device); does
+// not touch the context, which may already be destroyed.
+void imp_unet_destroy(imp_unet *u) { delete u; }
+
+long imp_unet_num_params(const imp_unet *u) { return u ? (long)u->net.n_params() : 0; }
+
+imp_status imp_unet_get_params(imp_unet *u, float *out) {
+    if (!u || !out) return fail(IMP_ERR_INVALID_ARG, "null argument");
+    imp_status s = imp::begin(u->ctx);
+    if (s != IMP_OK) return s;
+    IMP_CUDA(cudaMemcpyAsync(out, u->net.params(), u->net.n_params() * sizeof(float),
+                             cudaMemcpyDefault, u->ctx->stream),
+             "unet params D2H");
+    return imp::finish(u->ctx);
+}
+
+imp_status imp_unet_set_params(imp_unet *u, const float *in) {
+    if (!u || !in) return fail(IMP_ERR_INVALID_ARG, "null argument");
+    imp_status s = imp::begin(u->ctx);
+    if (s != IMP_OK) return s;
+    IMP_CUDA(cudaMemcpyAsync(u->net.params(), in, u->net.n_params() * sizeof(float),
+                             cudaMemcpyDefault, u->ctx->stream),
+             "unet params H2D");
+    IMP_CUDA(u->net.sync_weights(), "unet weights");
+    return imp::finish(u->ctx);
+}
+
+imp_status imp_unet_forward(imp_unet *u, const float *x, float *y) {
+    if (!u || !x || !y) return fail(IMP_ERR_INVALID_ARG, "null argument");
+    imp_status s = imp::begin(u->ctx);
+    if (s != IMP_OK) return s;
+    const size_t n = (size_t)u->net.batch() * 2 * u->net.height() * u->net.width();
+    DevKeep keep;
+    const float *dx;
+    float *dy;
+    bool yh;
+    if ((s = unet_io(u, x, n, keep, &dx)) || (s = imp::out_device(u->ctx, y, n, keep, &dy, &yh)))
+        return s;
+    IMP_CUDA(u->net.forward(dx, dy), "unet forward");
+    if (yh)
+        IMP_CUDA(cudaMemcpyAsync(y, dy, n * sizeof(float), cudaMemcpyDeviceToHost,
+                                 u->ctx->stream),
+                 "unet output D2H");
+    s = imp::finish(u->ctx);
+    u->ctx->launches = u->net.launches();
+    return s;
+}
+
+imp_status imp_unet_gradients(imp_unet *u, const float *x, const float *target, float *grads,
+                              float *loss) {
+    if (!u || !x || !target || !grads) return fail(IMP_ERR_INVALID_ARG, "null argument");
+    imp_status s = imp::begin(u->ctx);
+    if (s != IMP_OK) return s;
+    const size_t n = (size_t)u->net.batch() * 2 * u->net.height() * u->net.width();
+    DevKeep keep;
+    const float *dx, *dt;
+    if ((s = unet_io(u, x, n, keep, &dx)) || (s = unet_io(u, target, n, keep, &dt))) return s;
+    float l = 0.f;
+    IMP_CUDA(u->net.gradients(dx, dt, &l), "unet gradients");
+    IMP_CUDA(cudaMemcpyAsync(grads, u->net.grads(), u->net.n_params() * sizeof(float),
+                             cudaMemcpyDefault, u->ctx->stream),
+             "unet gradients D2H");
+    if (loss) *loss = l;
+    return imp::finish(u->ctx);
+}
+
+imp_status imp_unet_train_step(imp_unet *u, const float *x, const float *target, float lr,
+                               float *loss) {
+    if (!u || !x || !target) return fail(IMP_ERR_INVALID_ARG, "null argument");
+    if (!(lr > 0.f)) return fail(IMP_ERR_INVALID_ARG, "learning rate must be > 0");
+    imp_status s = imp::begin(u->ctx);
+    if (s != IMP_OK) return s;
+    const size_t n = (size_t)u->net.batch() * 2 * u->net.height() * u->net.width();
+    DevKeep keep;
+    const float *dx, *dt;
+    if ((s = unet_io(u, x, n, keep, &dx)) || (s = unet_io(u, target, n, keep, &dt))) return s;
+    float l = 0.f;
+    IMP_CUDA(u->net.train_step(dx, dt, lr, &l), "unet train step");
+    if (loss) *loss = l;
+    s = imp::finish(u->ctx);
+    u->ctx->launches = u->net.launches();
+    return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,227 @@
+"""Learned warm start for the Toeplitz CG (no counterpart in the reference).
+
+The problem is 2-D SENSE without a field map: a fixed spiral trajectory and
+coil set, F^H F applied through the library's Toeplitz operator, and CG on
+(F^H F + lambda D^H D) x = b with the reference's finite-difference penalty,
+lambda = rho * lambda_max(F^H F).  rho = 1e-3: without the penalty the
+converged least-squares image of noisy data is dominated by amplified noise,
+and with rho much below 1e-3 the condition number (~1/rho) times the FP32
+rounding reaches the 1e-3 NRMSE target itself.  With no field
+map every time-segment phase is 1, so Q is built with two Hanning segments
+(whose weights sum to one) and the two kernels are added: the single summed
+kernel is exactly F^H F's, and the CG then runs one segment.
+
+Training pairs come from the library's own solver: for a seeded phantom x,
+the right-hand side is b = F^H F x + F^H n (complex Gaussian k-space noise at
+the given SNR, gridded by the F^H d path) and the label is the plain
+50-iteration zero-start CG solution.  The U-Net maps b / rms(b) to
+label / (rms(b) kappa); kappa is the median label-to-input RMS ratio of the
+training set.  At test time the network output, rescaled, is the CG's
+starting image; plain zero-start CG is the fallback and the judge of its error.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import synth
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class ToepProblem:
+    """One fixed 2-D n x n trajectory and coil set resident on the GPU."""
+
+    def __init__(self, pkg, ctx, n: int, C: int, n_il: int, n_s: int, seed: int,
+                 os_q: float = 2.0, os_fh: float = 1.5, rho: float = 1e-3):
+        torch = _torch()
+        self.pkg, self.ctx, self.n, self.C = pkg, ctx, n, C
+        rng = np.random.default_rng(seed)
+        kx, ky, t = synth.spiral(n_il, n_s, n / 2 - 0.05, rng)
+        self.M, self.N = kx.size, n * n
+        sens = synth.coil_maps((n, n), C, rng, ring=True)
+        sens = np.stack([synth.to_voxel_order(s) for s in sens]).astype(np.complex64)
+        dev = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32)).cuda()
+        self.kx, self.ky, self.kz, self.t = dev(kx), dev(ky), dev(np.zeros_like(kx)), dev(t)
+        self.sr, self.si = dev(sens.real.ravel()), dev(sens.imag.ravel())
+        self.fm = torch.zeros(self.N, device="cuda")
+        G = 4 * n * n
+        self.o2 = pkg.toeplitz_options(ntime_segs=1, gridOS_Q=os_q, gridOS_FH=os_fh)
+        self.o1 = pkg.toeplitz_options(ntime_segs=0, gridOS_Q=os_q, gridOS_FH=os_fh)
+        qr = torch.zeros(2 * G, device="cuda")
+        qi = torch.zeros(2 * G, device="cuda")
+        pkg.toeplitz_q(ctx, self.o2, qr, qi, self.kx, self.ky, self.kz, self.t, self.M, n, n, 1)
+        self.qr = (qr[:G] + qr[G:]).contiguous()
+        self.qi = (qi[:G] + qi[G:]).contiguous()
+        # finite-difference penalty lambda = rho * lambda_max(F^H F) (power iteration)
+        v = torch.randn(2, self.N, device="cuda", generator=torch.Generator(
+            device="cuda").manual_seed(seed))
+        w = torch.zeros_like(v)
+        for _ in range(20):
+            v /= v.norm()
+            self.aha(v, w)
+            v, w = w, v
+        self.lmax = float(v.norm())
+        self.lam = rho * self.lmax
+        self.ocg = pkg.toeplitz_options(ntime_segs=0, gridOS_Q=os_q, gridOS_FH=os_fh,
+                                        fd_penalizer=self.lam)
+
+    # b = F^H F x  (x, out: [2][N] float32 CUDA tensors)
+    def aha(self, x, out):
+        self.pkg.toeplitz_apply(self.ctx, self.o1, out[0], out[1], x[0], x[1], self.qr, self.qi,
+                                self.t, self.M, self.fm, self.sr, self.si, self.C, self.n,
+                                self.n, 1)
+        return out
+
+    # F^H d for k-space data d [2][C*M]
+    def fhd(self, d, out):
+        self.pkg.toeplitz_fhd(self.ctx, self.o2, out[0], out[1], d[0], d[1], self.kx, self.ky,
+                              self.kz, self.t, self.fm, self.sr, self.si, self.M, self.C,
+                              self.n, self.n, 1)
+        return out
+
+    # CG on (F^H F + lambda D^H D) x = b from the image in x (overwritten);
+    # returns updates done
+    def cg(self, b, x, tol: float, max_iter: int) -> int:
+        return self.pkg.toeplitz_cg(self.ctx, self.ocg, x[0], x[1], b[0], b[1], self.qr, self.qi,
+                                    self.t, self.M, self.fm, self.sr, self.si, self.C, self.n,
+                                    self.n, 1, tol=tol, max_iter=max_iter)
+
+    def make_pairs(self, n_img: int, seed: int, snr_db: float = 40.0, label_iters: int = 50):
+        """(b [n][2][N], label [n][2][N], x_true [n][2][N]) on the GPU."""
+        torch = _torch()
+        rng = np.random.default_rng(seed)
+        n, N = self.n, self.N
+        xt = torch.zeros(n_img, 2, N, device="cuda")
+        for i in range(n_img):
+            img = synth.to_voxel_order(synth.ellipse_phantom((n, n), int(rng.integers(5, 16)), rng))
+            xt[i, 0] = torch.as_tensor(img.real.astype(np.float32))
+            xt[i, 1] = torch.as_tensor(img.imag.astype(np.float32))
+        b = torch.zeros_like(xt)
+        for i in range(n_img):  # one-segment operator
+            self.aha(xt[i], b[i])
+        # signal power per k-space sample: <x, F^H F x> / (C M)
+        power = (xt * b).sum(dim=(1, 2)) / (self.C * self.M)
+        sig = torch.sqrt(power / 10 ** (snr_db / 10) / 2)
+        noise = torch.zeros(2, self.C * self.M, device="cuda")
+        fhn = torch.zeros(2, N, device="cuda")
+        g = torch.Generator(device="cuda").manual_seed(seed)
+        for i in range(n_img):  # two-segment F^H d path
+            noise.normal_(generator=g)
+            noise *= sig[i]
+            self.fhd(noise, fhn)
+            b[i] += fhn
+        lab = torch.zeros_like(xt)
+        for i in range(n_img):
+            self.cg(b[i], lab[i], 0.0, label_iters)
+        return b, lab, xt
+
+
+def rms(a):
+    return a.pow(2).sum(dim=tuple(range(1, a.dim()))).div(a[0].numel() / 2).sqrt()
+
+
+def normalise(b, lab, kappa=None):
+    """inputs b / rms(b); targets label / (rms(b) kappa)."""
+    s = rms(b)
+    if kappa is None:
+        kappa = float((rms(lab) / s).median())
+    x = b / s.view(-1, 1, 1)
+    y = lab / (s * kappa).view(-1, 1, 1)
+    return x.contiguous(), y.contiguous(), kappa
+
+
+def train(net, inputs, targets, epochs: int, lr: float, seed: int = 0, log=None):
+    """Adam with cosine decay over minibatches of net.batch images."""
+    torch = _torch()
+    B = net.batch
+    n = inputs.shape[0]
+    steps = max(1, n // B) * epochs
+    g = torch.Generator().manual_seed(seed)
+    k = 0
+    losses = []
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=g)
+        ep_loss = []
+        for s in range(n // B):
+            idx = perm[s * B:(s + 1) * B].cuda()
+            lr_k = lr * 0.5 * (1.0 + np.cos(np.pi * k / steps))
+            ep_loss.append(net.train_step(inputs[idx].contiguous(), targets[idx].contiguous(),
+                                          max(lr_k, lr * 1e-3)))
+            k += 1
+        losses.append(float(np.mean(ep_loss)))
+        if log:
+            log(f"epoch {ep}: loss {losses[-1]:.5f}")
+    return losses
+
+
+def nrmse(a, ref):
+    return float((a - ref).norm() / ref.norm())
+
+
+def _cg_k(prob, b, x0, k):
+    x = x0.clone()
+    prob.cg(b, x, 0.0, k)
+    return x
+
+
+def iters_to_nrmse(prob, b, x0, ref, target: float, kmax: int) -> int:
+    """Smallest CG update count k <= kmax whose result is within `target`
+    NRMSE of ref (CG's error norm decreases monotonically; bisection)."""
+    if nrmse(x0, ref) <= target:
+        return 0
+    if nrmse(_cg_k(prob, b, x0, kmax), ref) > target:
+        return kmax + 1
+    lo, hi = 0, kmax
+    while hi - lo > 1:
+        mid = (lo + hi) // 2
+        if nrmse(_cg_k(prob, b, x0, mid), ref) <= target:
+            hi = mid
+        else:
+            lo = mid
+    return hi
+
+
+def evaluate(prob: ToepProblem, net1, kappa: float, b, target: float = 1e-3, tol: float = 1e-4,
+             kmax: int = 600, ref_iters: int = 1000):
+    """Warm versus zero start on each right-hand side in b ([n][2][N]).
+    net1: a batch-1 network.  Per image: CG updates and wall time to reach
+    NRMSE <= target against the converged solution (ref: CG to relative
+    residual 1e-6 or ref_iters updates), and updates to relative residual tol (the residual
+    test of toeplitz/recon.cu:2112)."""
+    torch = _torch()
+    out = []
+    for i in range(b.shape[0]):
+        bi = b[i].contiguous()
+        ref = torch.zeros_like(bi)
+        prob.cg(bi, ref, 1e-6, ref_iters)
+        zero = torch.zeros_like(bi)
+        s = float(rms(bi.unsqueeze(0))[0])
+        y = torch.zeros(1, 2, prob.N, device="cuda")
+        net1.forward((bi / s).unsqueeze(0).contiguous(), y)
+        xw0 = (y[0] * (s * kappa)).contiguous()
+        k_z = iters_to_nrmse(prob, bi, zero, ref, target, kmax)
+        k_w = iters_to_nrmse(prob, bi, xw0, ref, target, kmax)
+        # wall time of each path at its update count (network included)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        xz = _cg_k(prob, bi, zero, k_z)
+        torch.cuda.synchronize()
+        t_z = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        net1.forward((bi / s).unsqueeze(0).contiguous(), y)
+        xw = _cg_k(prob, bi, (y[0] * (s * kappa)).contiguous(), k_w)
+        torch.cuda.synchronize()
+        t_w = time.perf_counter() - t0
+        xr = zero.clone()
+        it_rz = prob.cg(bi, xr, tol, kmax)
+        xr = xw0.clone()
+        it_rw = prob.cg(bi, xr, tol, kmax)
+        out.append(dict(zero_iters=k_z, zero_s=t_z, zero_nrmse=nrmse(xz, ref), warm_iters=k_w,
+                        warm_s=t_w, warm_nrmse=nrmse(xw, ref), x0_nrmse=nrmse(xw0, ref),
+                        zero_iters_tol=it_rz, warm_iters_tol=it_rw))
+    return out

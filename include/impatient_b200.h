@@ -232,6 +232,43 @@ imp_status imp_toeplitz_apply(imp_context *ctx, const imp_toeplitz_options *opt,
                               const float *fm, const float *sensi_r, const float *sensi_i,
                               int num_coil, int nx, int ny, int nz);
 
+/* Toeplitz CG started from the image in x (the warm start) and stopped when
+ * sqrt(|r|^2 / |F^H d|^2) < tol (the residual test of toeplitz/recon.cu:2112)
+ * or after max_iter updates; x receives the minimum-residual iterate and
+ * *iterations (optional) the updates performed.  FD regularization as in opt;
+ * no TV passes.  No counterpart in the reference (which always starts from
+ * zero, toeplitz/recon.cu:1871): it is the CG half of the learned warm start. */
+imp_status imp_toeplitz_cg(imp_context *ctx, const imp_toeplitz_options *opt, float *x_r,
+                           float *x_i, const float *fhd_r, const float *fhd_i, const float *q_r,
+                           const float *q_i, const float *t, int num_k, const float *fm,
+                           const float *sensi_r, const float *sensi_i, int num_coil, int nx,
+                           int ny, int nz, double tol, int max_iter, int *iterations);
+
+/* ---- Learned warm start: BF16 U-Net (no counterpart in the reference) ----
+ * 2 channels (re, im) in and out, 4 levels of 32-256 channels, 3x3 convs with
+ * ReLU, max-pool down, nearest x2 + 1x1 conv up, skip concatenation; BF16
+ * weights and activations with FP32 accumulation on the tensor cores, FP32
+ * master weights and Adam.  Images are [batch][2][height*width] float32,
+ * height and width multiples of 8; pointers may be host or device. */
+typedef struct imp_unet imp_unet;
+
+imp_status imp_unet_create(imp_context *ctx, int batch, int height, int width,
+                           unsigned long long seed, imp_unet **out);
+void imp_unet_destroy(imp_unet *net);
+long imp_unet_num_params(const imp_unet *net);
+/* FP32 parameters, per layer weights [cout][ky][kx][cin] then bias [cout]. */
+imp_status imp_unet_get_params(imp_unet *net, float *params);
+imp_status imp_unet_set_params(imp_unet *net, const float *params);
+imp_status imp_unet_forward(imp_unet *net, const float *x, float *y);
+/* Gradients (same layout as the parameters) of the mean squared error between
+ * forward(x) and target, without an update; *loss (optional) gets the error. */
+imp_status imp_unet_gradients(imp_unet *net, const float *x, const float *target, float *grads,
+                              float *loss);
+/* One Adam step (lr) on the mean squared error between forward(x) and target;
+ * *loss (optional) receives that error before the step. */
+imp_status imp_unet_train_step(imp_unet *net, const float *x, const float *target, float lr,
+                               float *loss);
+
 /* Directory-level drop-in of toeplitz(idir, ...) (main_mri.cuh:97-108,
  * main_mri.cu:207-630): Q by gridding, by direct evaluation (direct != 0)
  * or read from Qdir/Q_stone.file (reuseQ != 0; Qdir NULL = idir), F^H d,

@@ -1,0 +1,98 @@
+"""The learned warm start's BF16 U-Net on the GPU against its float64 torch-CPU
+oracle (oracle/unet.py), through the C-ABI.
+
+Tolerances (relative L2): the forward pass within 1e-2 of the oracle that
+rounds to BF16 where the network stores BF16 (the rest is FP32 versus FP64
+accumulation); the loss within 1e-2 and every layer's weight gradient within
+1e-1 (the backward pass also carries BF16 output gradients into the GEMMs)."""
+import numpy as np
+import pytest
+
+from oracle import unet as U
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(pkg):
+    c = pkg.Context(0)
+    yield c
+    c.close()
+
+
+def rel(a, b):
+    return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / np.linalg.norm(np.ravel(b)))
+
+
+def data(B, H, W, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((B, 2, H * W)).astype(np.float32)
+    t = (0.5 * x + 0.1 * rng.standard_normal(x.shape)).astype(np.float32)
+    return x, t
+
+
+def test_param_count_and_roundtrip(pkg, ctx):
+    net = pkg.UNet(ctx, 1, 16, 16, seed=3)
+    try:
+        assert net.num_params() == U.n_params()
+        p = net.get_params()
+        q = p.copy()
+        q[::7] += 0.25
+        net.set_params(q)
+        assert np.array_equal(net.get_params(), q)
+    finally:
+        net.close()
+
+
+def test_forward_matches_oracle(pkg, ctx):
+    B, H, W = 2, 32, 48
+    net = pkg.UNet(ctx, B, H, W, seed=11)
+    p = net.get_params()
+    x, _ = data(B, H, W, 1)
+    y = net.forward(x, np.zeros_like(x))
+    want, _ = U.forward(p, x, H, W, emulate_bf16=True)
+    exact, _ = U.forward(p, x, H, W, emulate_bf16=False)
+    net.close()
+    e, e64 = rel(y, want.detach().numpy()), rel(y, exact.detach().numpy())
+    print(f"forward vs BF16-emulating oracle {e:.2e}, vs float64 oracle {e64:.2e}")
+    assert e < 1e-2
+
+
+def test_gradients_match_oracle(pkg, ctx):
+    B, H, W = 2, 32, 32
+    net = pkg.UNet(ctx, B, H, W, seed=12)
+    p = net.get_params()
+    x, t = data(B, H, W, 2)
+    loss, g = net.gradients(x, t)
+    loss_o, g_o = U.loss_and_grads(p, x, t, H, W, emulate_bf16=True)
+    assert abs(loss - loss_o) / loss_o < 1e-2
+    worst, errs = 0.0, []
+    for i, (a, b) in enumerate(U.layer_slices()):
+        ref = g_o[a:b]
+        if i == 0:  # only the two real input channels of the first layer carry gradient
+            ref = ref.reshape(32, 9, 16)[:, :, :2]
+            got = g[a:b].reshape(32, 9, 16)[:, :, :2]
+        elif i == len(U.CFG) - 1:  # only outputs 0 and 1 of the last layer
+            ref = ref.reshape(16, 32)[:2]
+            got = g[a:b].reshape(16, 32)[:2]
+        else:
+            got = g[a:b]
+        e = rel(got, ref)
+        worst = max(worst, e)
+        errs.append(e)
+    net.close()
+    print(f"loss {loss:.6f} vs {loss_o:.6f}; layer weight-gradient errors "
+          + " ".join(f"{e:.1e}" for e in errs))
+    assert worst < 1e-1
+
+
+def test_training_reduces_loss(pkg, ctx):
+    B, H, W = 4, 32, 32
+    net = pkg.UNet(ctx, B, H, W, seed=13)
+    x, t = data(B, H, W, 3)
+    try:
+        losses = [net.train_step(x, t, 2e-3) for _ in range(80)]
+    finally:
+        net.close()
+    print(f"loss {losses[0]:.4f} -> {losses[-1]:.4f}")
+    assert losses[-1] < 0.2 * losses[0]
