@@ -547,6 +547,189 @@ def run_toep_apply_only(args, local):
     return 0
 
 
+# ---------------------------------------------------------- warm start --
+
+WARM = "warm512"
+WARM_METRIC = ("s/recon to NRMSE<=1e-3 vs converged CG (2-D 512x512, 32 coils, Toeplitz CG): "
+               "learned warm start (value) vs zero start")
+WEIGHTS = ROOT / "impatient-mri_b200" / "weights" / "unet_warm512.npz"
+
+
+def run_warm(args, local):
+    """Learned warm start at the configuration's size: 2-D 512x512, 32 coils
+    on a ring, 24 x 4096 spiral (M = 98304), no field map, CG with the finite-
+    difference penalty lambda = 1e-3 lambda_max, 40 dB noise.  Trains the
+    U-Net on seeded phantoms with 50-iteration CG labels unless trained
+    weights are present, then times CG from the network output and from zero
+    on held-out phantoms."""
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from impatient_mri_b200 import learn
+    torch.cuda.set_device(local)
+    ctx = pkg.Context(local)
+    log = lambda m: print(m, file=sys.stderr, flush=True)
+    t0 = time.perf_counter()
+    prob = learn.ToepProblem(pkg, ctx, n=512, C=32, n_il=24, n_s=4096, seed=1005)
+    log(f"problem setup {time.perf_counter() - t0:.1f} s, lambda {prob.lam:.4g}")
+    trained_here = False
+    if WEIGHTS.exists() and not args.retrain:
+        params, kappa, meta = learn.load_weights(WEIGHTS)
+        train_info = {k: v.tolist() for k, v in meta.items()}
+    else:
+        t0 = time.perf_counter()
+        b, lab, _ = prob.make_pairs(args.train_images, seed=2005)
+        t_pairs = time.perf_counter() - t0
+        x, y, kappa = learn.normalise(b, lab)
+        del b, lab
+        net = pkg.UNet(ctx, args.batch, 512, 512, seed=7)
+        t0 = time.perf_counter()
+        losses = learn.train(net, x, y, epochs=args.epochs, lr=args.lr, log=log)
+        t_train = time.perf_counter() - t0
+        params = net.get_params()
+        net.close()
+        del x, y
+        train_info = dict(train_images=args.train_images, epochs=args.epochs, lr=args.lr,
+                          batch=args.batch, final_loss=losses[-1], pairs_s=t_pairs,
+                          train_s=t_train)
+        out = ROOT / "gpurun_out" / "unet_warm512.npz"
+        out.parent.mkdir(exist_ok=True)
+        learn.save_weights(out, params, kappa, train_info)
+        trained_here = True
+    net1 = pkg.UNet(ctx, 1, 512, 512, seed=7)
+    net1.set_params(params)
+    bt, _, _ = prob.make_pairs(args.test_images, seed=3005)
+    for _ in range(max(args.warmup, 1)):  # warm the graphs and the network
+        learn.evaluate(prob, net1, kappa, bt[:1], target=1e-3, kmax=200)
+    res = learn.evaluate(prob, net1, kappa, bt, target=1e-3, kmax=200)
+    f = lambda k: float(np.mean([r[k] for r in res]))
+    line = {
+        "metric": WARM_METRIC, "value": f("warm_s"), "unit": UNIT, "n_gpus": 1,
+        "steps": len(res), "warmup": args.warmup, "ms_per_step": f("warm_s") * 1e3,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16",
+        "data": "synthetic (seeded ellipse phantoms, ring coils, spiral; 40 dB k-space noise)",
+        "config": {"workload": f"{WARM}: 512x512, 32 coils, 24 x 4096 spiral, no field map, "
+                               f"FD lambda = 1e-3 lambda_max ({prob.lam:.4g}), U-Net 2->2 ch, "
+                               f"4 levels 32-256 ch, BF16", "train": train_info,
+                   "trained_in_this_run": trained_here},
+        "zero_start": {"s_per_recon": f("zero_s"), "cg_updates": f("zero_iters"),
+                       "nrmse": f("zero_nrmse"), "cg_updates_to_residual_1e-4":
+                           f("zero_iters_tol")},
+        "warm_start": {"s_per_recon": f("warm_s"), "cg_updates": f("warm_iters"),
+                       "nrmse": f("warm_nrmse"), "start_nrmse": f("x0_nrmse"),
+                       "cg_updates_to_residual_1e-4": f("warm_iters_tol")},
+        "speedup": f("zero_s") / f("warm_s"),
+    }
+    net1.close()
+    ctx.close()
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------- multi-slice --
+
+BATCH = "batch384"
+BATCH_METRIC = ("s/recon (brute-force CG, 64 independent 2-D 384x384 slices, 32 coils, "
+                "16-32 x 4096-sample spirals per slice, 20 CG iterations)")
+
+
+def run_batch(args, local):
+    """Configuration 4: independent 384x384 slices with 32 ring coils, each with
+    its own seeded spiral of 16..32 interleaves x 4096 samples (uneven M), field
+    map and phantom; plain CG, cg_num 20 (19 updates).  All slices go through
+    one imp_bruteforce_batch call.  The timed job is the first `--slices`
+    slices of the seeded 64; value = its time x 64 / slices (extrapolated,
+    stated in config)."""
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from impatient_mri_b200 import synth
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = pkg.Context(local)
+    n, C, S_total = 384, 32, 64
+    S = max(1, min(args.slices, S_total))
+    rng = np.random.default_rng(1004)
+    ix, iy, iz = synth.grid_positions(n, n, 1)
+    sens = np.stack([synth.to_voxel_order(m)
+                     for m in synth.coil_maps((n, n), C, rng, ring=True)]).astype(np.complex64)
+    N = n * n
+    f = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32)).to(dev)
+    D = dict(ix=f(ix), iy=f(iy), iz=f(iz), sr=f(sens.real.ravel()), si=f(sens.imag.ravel()))
+    kx, ky, tt, fms, kdr, kdi, ms = [], [], [], [], [], [], []
+    for s_ in range(S_total):
+        il = int(rng.integers(16, 33))
+        skx, sky, st = synth.spiral(il, 4096, n / 2 - 0.05, rng)
+        img = synth.to_voxel_order(synth.ellipse_phantom((n, n), 8, rng))
+        fm = synth.to_voxel_order(synth.field_map((n, n), rng)).astype(np.float32)
+        ms.append(skx.size)
+        if s_ >= S:
+            continue
+        M = skx.size
+        yr = torch.zeros(C * M, device=dev)
+        yi = torch.zeros(C * M, device=dev)
+        g = dict(kx=f(skx), ky=f(sky), kz=f(np.zeros_like(skx)), t=f(st), fm=f(fm))
+        pkg.parallelFtGpu(ctx, yr, yi, f(img.real), f(img.imag), g["kx"], g["ky"], g["kz"],
+                          D["ix"], D["iy"], D["iz"], g["fm"], g["t"], M, N, D["sr"], D["si"], C, 0)
+        y = yr.cpu().numpy() + 1j * yi.cpu().numpy()
+        y = synth.add_noise(y, 40.0, rng).astype(np.complex64)
+        kx.append(skx); ky.append(sky); tt.append(st); fms.append(fm)
+        kdr.append(y.real.astype(np.float32)); kdi.append(y.imag.astype(np.float32))
+    k_off = np.cumsum([0] + ms[:S])
+    B = dict(kx=f(np.concatenate(kx)), ky=f(np.concatenate(ky)),
+             kz=f(np.zeros(int(k_off[-1]), np.float32)), t=f(np.concatenate(tt)),
+             fm=f(np.concatenate(fms)), kr=f(np.concatenate(kdr)), ki=f(np.concatenate(kdi)))
+    xr = torch.zeros(S * N, device=dev)
+    xi = torch.zeros(S * N, device=dev)
+    opts = pkg.bf_options(cg_num=20)
+
+    def recon():
+        xr.zero_(); xi.zero_()
+        pkg.bruteForceBatch(ctx, opts, xr, xi, B["kr"], B["ki"], B["kx"], B["ky"], B["kz"],
+                            B["t"], k_off, D["ix"], D["iy"], D["iz"], B["fm"], D["sr"], D["si"],
+                            N, C)
+
+    for _ in range(max(args.warmup, 1)):
+        recon()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    launches = 0
+    with ClockSampler(local) as clk:
+        for s_ in range(args.steps):
+            ev[s_][0].record()
+            recon()
+            ev[s_][1].record()
+            launches += ctx.launch_count()
+    torch.cuda.synchronize()
+    ms_step = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    pairs = float(sum(ms[:S])) * N
+    applies = 1 + 2 * 19
+    flop = 2.0 * (3 + 4 * C) * pairs * applies
+    achieved = flop / (ms_step / 1e3) / 1e12
+    fp32_peak, _ = pkg.measure_alu_peaks(local)
+    line = {
+        "metric": BATCH_METRIC, "value": ms_step / 1e3 * S_total / S, "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded spirals, phantoms, field maps, ring coils; 40 dB noise)",
+        "config": {"workload": f"{BATCH}: {S} of 64 slices timed (sample counts "
+                               f"{ms[:S]}), value extrapolated x{S_total / S:.1f}; 384x384, "
+                               f"32 coils, cg_num 20, no regularization",
+                   "parallelism": "one imp_bruteforce_batch call, solver cached per sample "
+                                  "count"},
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak, "traffic": None,
+                     "kernel": "whole recon (NUDFT F and F^H dominate): algorithmic FLOP "
+                               "2 (3 + 4C) per (sample, voxel) pair per apply, 39 applies"},
+        "clocks": clk.summary(),
+    }
+    ctx.close()
+    print(json.dumps(line))
+    return 0
+
+
 def run_nudft_only(args, local):
     """Forward + adjoint NUDFT applies of the benchmark geometry through the
     operator C-ABI (the small command the kernel profiles are taken on)."""
@@ -586,8 +769,16 @@ def main() -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, TOEP],
-                    help="bf3d_64x64x16 (default, the headline) or the Toeplitz 3-D case")
+    ap.add_argument("--slices", type=int, default=4, help="batch384: slices timed")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, TOEP, WARM, BATCH],
+                    help="bf3d_64x64x16 (default, the headline), the Toeplitz 3-D case, or "
+                         "the learned warm start at 512x512 with 32 coils")
+    ap.add_argument("--retrain", action="store_true", help="warm512: train even if weights exist")
+    ap.add_argument("--train-images", type=int, default=2000)
+    ap.add_argument("--test-images", type=int, default=8)
+    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=1e-3)
     args = ap.parse_args()
     ws, rank, local = dist_setup()
     try:
@@ -599,6 +790,10 @@ def main() -> int:
             return run_reference(args, ws, rank)
         if args.workload == TOEP:
             return run_toeplitz(args, ws, rank, local)
+        if args.workload == WARM:
+            return run_warm(args, local)
+        if args.workload == BATCH:
+            return run_batch(args, local)
         return run_ours(args, ws, rank, local)
     finally:
         if ws > 1:

@@ -40,6 +40,7 @@ EXPORTED = [
     "imp_context_launch_count", "imp_context_profile", "imp_context_profile_read",
     "imp_ft", "imp_ift", "imp_parallel_ft", "imp_parallel_ift", "imp_parallel_ift_noalloc",
     "imp_bf_options_default", "imp_bruteforce_recon", "imp_bruteforce_dir",
+    "imp_bruteforce_batch",
     "imp_dataset_info", "imp_mrisolver_main", "imp_measure_alu_peaks",
     "imp_toeplitz_options_default", "imp_toeplitz_q", "imp_toeplitz_fhd", "imp_toeplitz_recon",
     "imp_toeplitz_apply", "imp_toeplitz_dir", "imp_toeplitz_cg",
@@ -104,6 +105,8 @@ def lib() -> ctypes.CDLL:
         L.imp_bf_options_default.argtypes = [ctypes.POINTER(BfOptions)]
         L.imp_bruteforce_recon.argtypes = ([vp, ctypes.POINTER(BfOptions)] + [vp] * 14
                                            + [ip, ip, ip, ip])
+        L.imp_bruteforce_batch.argtypes = ([vp, ctypes.POINTER(BfOptions)] + [vp] * 8
+                                           + [ctypes.POINTER(ip)] + [vp] * 6 + [ip, ip, ip])
         L.imp_bruteforce_dir.argtypes = [ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.POINTER(BfOptions), ip]
         L.imp_dataset_info.argtypes = [ctypes.c_char_p] + [ctypes.POINTER(ctypes.c_int)] * 7
@@ -253,6 +256,19 @@ def bruteForceGpu(ctx, opts: BfOptions, idata_r, idata_i, kdata_r, kdata_i, kx, 
         ctx.handle, ctypes.byref(opts), *map(_ptr, (idata_r, idata_i, kdata_r, kdata_i, kx, ky,
                                                     kz, ix, iy, iz, fm, t, sensi_r, sensi_i)),
         num_k, num_i, num_coil, num_slices))
+
+
+def bruteForceBatch(ctx, opts: BfOptions, idata_r, idata_i, kdata_r, kdata_i, kx, ky, kz, t,
+                    k_off, ix, iy, iz, fm, sensi_r, sensi_i, num_i, num_coil):
+    """Slices with their own trajectories: k_off (num_slices+1 offsets into the
+    concatenated kx/ky/kz/t); kdata slice-major, coil-major within a slice;
+    idata/fm [slice][num_i].  idata_* hold the initial estimates and receive
+    the images."""
+    off = (ctypes.c_int * len(k_off))(*[int(v) for v in k_off])
+    _check(lib().imp_bruteforce_batch(
+        ctx.handle, ctypes.byref(opts), *map(_ptr, (idata_r, idata_i, kdata_r, kdata_i, kx, ky,
+                                                    kz, t)),
+        off, *map(_ptr, (ix, iy, iz, fm, sensi_r, sensi_i)), num_i, num_coil, len(k_off) - 1))
 
 
 def bruteForce(idir: str, odir: str, opts: BfOptions, gpu_id: int = 0) -> None:

@@ -247,6 +247,7 @@ imp_status imp_context_destroy(imp_context *ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->bf.reset();
+    ctx->bf_by_m.clear();
     ctx->tp.reset();
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->dev_err) cudaFree(ctx->dev_err);
@@ -307,6 +308,43 @@ void imp_bf_options_default(imp_bf_options *opt) {
     opt->tv_eps = 1e-6f;
 }
 
+// BfConfig of one brute-force problem from the C options (TV grid as the
+// reference: sqrt(N) x sqrt(N) unless nx, ny, nz are given).
+static imp_status bf_config(const imp_bf_options *opt, int num_k, int num_i, int num_coil,
+                     imp::BfConfig *cfg) {
+    cfg->M = num_k;
+    cfg->N = num_i;
+    cfg->C = num_coil;
+    cfg->use_z = opt->use_z != 0;
+    cfg->cg_num = opt->cg_num;
+    cfg->fd = opt->enable_fd != 0;
+    cfg->lambda = opt->fd_penalizer;
+    cfg->tv = opt->enable_tv != 0;
+    cfg->tv_num = opt->enable_tv ? opt->tv_num : 1;
+    cfg->tv_eps = opt->tv_eps;
+    if (opt->nx == 0 && opt->ny == 0 && opt->nz == 0) {
+        // the reference's 2-D TV grid of side sqrt(N) (bruteForceGpu.cu:446-451)
+        const int side = (int)std::lround(std::sqrt((double)num_i));
+        if ((cfg->fd || cfg->tv) && side * side != num_i)
+            return fail(IMP_ERR_INVALID_ARG, "TV on a sqrt(N) x sqrt(N) grid needs square N");
+        cfg->n0 = side;
+        cfg->n1 = side;
+        cfg->n2 = 1;
+        if (side * side != num_i) {
+            cfg->n0 = num_i;
+            cfg->n1 = 1;
+        }
+    } else {
+        if (opt->nx <= 0 || opt->ny <= 0 || opt->nz <= 0 ||
+            (long)opt->nx * opt->ny * opt->nz != num_i)
+            return fail(IMP_ERR_INVALID_ARG, "nx*ny*nz must equal num_i");
+        cfg->n0 = opt->ny;  // (y, x, z) with z fastest
+        cfg->n1 = opt->nx;
+        cfg->n2 = opt->nz;
+    }
+    return IMP_OK;
+}
+
 imp_status imp_bruteforce_recon(imp_context *ctx, const imp_bf_options *opt, float *idata_r,
                                 float *idata_i, const float *kdata_r, const float *kdata_i,
                                 const float *kx, const float *ky, const float *kz,
@@ -325,36 +363,7 @@ imp_status imp_bruteforce_recon(imp_context *ctx, const imp_bf_options *opt, flo
     if (opt->cg_num <= 0) return fail(IMP_ERR_INVALID_ARG, "cg_num must be > 0");
     if (opt->enable_tv && opt->tv_num <= 0) return fail(IMP_ERR_INVALID_ARG, "tv_num must be > 0");
     imp::BfConfig cfg;
-    cfg.M = num_k;
-    cfg.N = num_i;
-    cfg.C = num_coil;
-    cfg.use_z = opt->use_z != 0;
-    cfg.cg_num = opt->cg_num;
-    cfg.fd = opt->enable_fd != 0;
-    cfg.lambda = opt->fd_penalizer;
-    cfg.tv = opt->enable_tv != 0;
-    cfg.tv_num = opt->enable_tv ? opt->tv_num : 1;
-    cfg.tv_eps = opt->tv_eps;
-    if (opt->nx == 0 && opt->ny == 0 && opt->nz == 0) {
-        // the reference's 2-D TV grid of side sqrt(N) (bruteForceGpu.cu:446-451)
-        const int side = (int)std::lround(std::sqrt((double)num_i));
-        if ((cfg.fd || cfg.tv) && side * side != num_i)
-            return fail(IMP_ERR_INVALID_ARG, "TV on a sqrt(N) x sqrt(N) grid needs square N");
-        cfg.n0 = side;
-        cfg.n1 = side;
-        cfg.n2 = 1;
-        if (side * side != num_i) {
-            cfg.n0 = num_i;
-            cfg.n1 = 1;
-        }
-    } else {
-        if (opt->nx <= 0 || opt->ny <= 0 || opt->nz <= 0 ||
-            (long)opt->nx * opt->ny * opt->nz != num_i)
-            return fail(IMP_ERR_INVALID_ARG, "nx*ny*nz must equal num_i");
-        cfg.n0 = opt->ny;  // (y, x, z) with z fastest
-        cfg.n1 = opt->nx;
-        cfg.n2 = opt->nz;
-    }
+    if ((s = bf_config(opt, num_k, num_i, num_coil, &cfg)) != IMP_OK) return s;
     if ((s = begin(ctx)) != IMP_OK) return s;
     std::vector<std::unique_ptr<void, void (*)(void *)>> keep;
     const size_t M = num_k, N = num_i, C = num_coil, S = num_slices;
@@ -409,6 +418,85 @@ imp_status imp_bruteforce_recon(imp_context *ctx, const imp_bf_options *opt, flo
     ctx->launches = launches;
     if (s == IMP_OK && ctx->prof_on)
         IMP_CUDA(solver.profile_collect(ctx->prof_ms, ctx->prof_count), "profile collect");
+    return s;
+}
+
+imp_status imp_bruteforce_batch(imp_context *ctx, const imp_bf_options *opt, float *idata_r,
+                                float *idata_i, const float *kdata_r, const float *kdata_i,
+                                const float *kx, const float *ky, const float *kz,
+                                const float *t, const int *k_off, const float *ix,
+                                const float *iy, const float *iz, const float *fm,
+                                const float *sensi_r, const float *sensi_i, int num_i,
+                                int num_coil, int num_slices) {
+    if (!opt || !k_off) return fail(IMP_ERR_INVALID_ARG, "null options or offsets");
+    if (num_slices <= 0 || num_coil <= 0 || num_i <= 0)
+        return fail(IMP_ERR_INVALID_ARG, "num_slices, num_coil and num_i must be > 0");
+    if (k_off[0] != 0) return fail(IMP_ERR_INVALID_ARG, "k_off[0] must be 0");
+    for (int sl = 0; sl < num_slices; ++sl)
+        if (k_off[sl + 1] <= k_off[sl])
+            return fail(IMP_ERR_INVALID_ARG, "every slice needs at least one sample");
+    const size_t Mt = (size_t)k_off[num_slices];
+    imp_status s = check_op_args(idata_r, idata_i, kdata_r, kdata_i, kx, ky, ix, iy, t,
+                                 (int)std::min<size_t>(Mt, INT32_MAX), num_i, opt->use_z, kz, iz);
+    if (s != IMP_OK) return s;
+    if (num_coil > 1 && (!sensi_r || !sensi_i))
+        return fail(IMP_ERR_INVALID_ARG, "sensi needed for num_coil > 1");
+    if (opt->cg_num <= 0) return fail(IMP_ERR_INVALID_ARG, "cg_num must be > 0");
+    if (opt->enable_tv && opt->tv_num <= 0) return fail(IMP_ERR_INVALID_ARG, "tv_num must be > 0");
+    if ((s = begin(ctx)) != IMP_OK) return s;
+    std::vector<std::unique_ptr<void, void (*)(void *)>> keep;
+    const size_t N = num_i, C = num_coil, S = num_slices;
+    const float *d_kx, *d_ky, *d_kz = nullptr, *d_ix, *d_iy, *d_iz = nullptr, *d_t, *d_fm = nullptr;
+    const float *d_sr = nullptr, *d_si = nullptr, *d_kr, *d_ki, *d_xr0, *d_xi0;
+    bool x_host = false, dummy;
+    if ((s = to_device(ctx, kx, Mt, keep, &d_kx, &dummy)) ||
+        (s = to_device(ctx, ky, Mt, keep, &d_ky, &dummy)) ||
+        (s = to_device(ctx, kz, Mt, keep, &d_kz, &dummy)) ||
+        (s = to_device(ctx, t, Mt, keep, &d_t, &dummy)) ||
+        (s = to_device(ctx, ix, N, keep, &d_ix, &dummy)) ||
+        (s = to_device(ctx, iy, N, keep, &d_iy, &dummy)) ||
+        (s = to_device(ctx, iz, N, keep, &d_iz, &dummy)) ||
+        (s = to_device(ctx, fm, S * N, keep, &d_fm, &dummy)) ||
+        (s = to_device(ctx, sensi_r, C * N, keep, &d_sr, &dummy)) ||
+        (s = to_device(ctx, sensi_i, C * N, keep, &d_si, &dummy)) ||
+        (s = to_device(ctx, kdata_r, C * Mt, keep, &d_kr, &dummy)) ||
+        (s = to_device(ctx, kdata_i, C * Mt, keep, &d_ki, &dummy)) ||
+        (s = to_device(ctx, idata_r, S * N, keep, &d_xr0, &x_host)) ||
+        (s = to_device(ctx, idata_i, S * N, keep, &d_xi0, &dummy)))
+        return s;
+    float *d_xr = const_cast<float *>(d_xr0), *d_xi = const_cast<float *>(d_xi0);
+    if (num_coil == 1) {
+        d_sr = nullptr;  // one coil: unit sensitivity (kernels/structures.cpp:710-716)
+        d_si = nullptr;
+    }
+    long launches = 0;
+    for (int sl = 0; sl < num_slices; ++sl) {
+        const int Ms = k_off[sl + 1] - k_off[sl];
+        imp::BfConfig cfg;
+        if ((s = bf_config(opt, Ms, num_i, num_coil, &cfg)) != IMP_OK) return s;
+        // one solver per sample count: buffers, tuned shapes and graphs are
+        // reused by every slice of that size (and by later calls)
+        std::unique_ptr<imp::BfSolver> &slot = ctx->bf_by_m[Ms];
+        if (!slot) slot.reset(new imp::BfSolver());
+        const size_t o = (size_t)k_off[sl];
+        IMP_CUDA(slot->setup(cfg, d_kx + o, d_ky + o, d_kz ? d_kz + o : nullptr, d_t + o, d_ix,
+                             d_iy, d_iz, d_sr, d_si, ctx->dev_err, ctx->stream),
+                 "brute-force setup");
+        IMP_CUDA(slot->solve(d_fm ? d_fm + (size_t)sl * N : nullptr, d_kr + C * o, d_ki + C * o,
+                             d_xr + (size_t)sl * N, d_xi + (size_t)sl * N),
+                 "brute-force solve");
+        launches += slot->launches() + 4;
+    }
+    if (x_host) {
+        IMP_CUDA(cudaMemcpyAsync(idata_r, d_xr, S * N * sizeof(float), cudaMemcpyDeviceToHost,
+                                 ctx->stream),
+                 "output D2H");
+        IMP_CUDA(cudaMemcpyAsync(idata_i, d_xi, S * N * sizeof(float), cudaMemcpyDeviceToHost,
+                                 ctx->stream),
+                 "output D2H");
+    }
+    s = finish(ctx);
+    ctx->launches = launches;
     return s;
 }
 

@@ -3,6 +3,7 @@
 #include "../../include/impatient_b200.h"
 
 #include <cuda_runtime.h>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -23,6 +24,7 @@ struct imp_context {
     double prof_ms[2] = {0.0, 0.0};
     long prof_count[2] = {0, 0};
     std::unique_ptr<imp::BfSolver> bf;    // brute-force solver reused across calls
+    std::map<int, std::unique_ptr<imp::BfSolver>> bf_by_m;  // batched slices, per sample count
     std::unique_ptr<imp::ToepSolver> tp;  // Toeplitz solver reused across calls
     ~imp_context();
 };

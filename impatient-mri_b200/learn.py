@@ -225,3 +225,19 @@ def evaluate(prob: ToepProblem, net1, kappa: float, b, target: float = 1e-3, tol
                         warm_s=t_w, warm_nrmse=nrmse(xw, ref), x0_nrmse=nrmse(xw0, ref),
                         zero_iters_tol=it_rz, warm_iters_tol=it_rw))
     return out
+
+
+def save_weights(path, params, kappa: float, meta: dict):
+    """Parameters stored as bfloat16 bit patterns (the precision the network
+    computes in), with kappa and the training configuration."""
+    p = np.asarray(params, np.float32)
+    bits = (p.view(np.uint32) + 0x7FFF + ((p.view(np.uint32) >> 16) & 1)) >> 16
+    np.savez_compressed(path, bf16=bits.astype(np.uint16), kappa=np.float64(kappa),
+                        **{k: np.asarray(v) for k, v in meta.items()})
+
+
+def load_weights(path):
+    z = np.load(path)
+    params = (z["bf16"].astype(np.uint32) << 16).view(np.float32)
+    meta = {k: z[k] for k in z.files if k not in ("bf16", "kappa")}
+    return params, float(z["kappa"]), meta

@@ -159,6 +159,23 @@ imp_status imp_bruteforce_recon(imp_context *ctx, const imp_bf_options *opt, flo
                                 const float *sensi_i, int num_k, int num_i, int num_coil,
                                 int num_slices);
 
+/* Brute-force CG recon of num_slices slices that share the image grid
+ * (ix, iy, iz: num_i) and the coil maps but each have their own trajectory and
+ * sample count (uneven M), k-space data and field map -- the multi-slice loop
+ * of main_mri.cu:875-895 generalised to per-slice trajectories.  Slice s owns
+ * samples k_off[s] .. k_off[s+1]-1 of kx, ky, kz, t (k_off: host array of
+ * num_slices+1 offsets, k_off[0] = 0); its data are
+ * kdata[num_coil*k_off[s] + c*(k_off[s+1]-k_off[s]) + k]; fm and idata are
+ * [slice][num_i].  The context keeps one solver per distinct sample count, so
+ * buffers, tuned shapes and CUDA graphs are reused by every slice of that size. */
+imp_status imp_bruteforce_batch(imp_context *ctx, const imp_bf_options *opt, float *idata_r,
+                                float *idata_i, const float *kdata_r, const float *kdata_i,
+                                const float *kx, const float *ky, const float *kz,
+                                const float *t, const int *k_off, const float *ix,
+                                const float *iy, const float *iz, const float *fm,
+                                const float *sensi_r, const float *sensi_i, int num_i,
+                                int num_coil, int num_slices);
+
 /* Directory-level drop-in of bruteForce(idir, odir, ...) (main_mri.cuh:110-118,
  * main_mri.cu:652-1025): reads idir in the 0.2 or 1.0 format
  * (kernels/structures.cpp:569-1162), reconstructs every slice and writes

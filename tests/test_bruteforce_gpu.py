@@ -145,3 +145,40 @@ def test_cli_end_to_end(pkg, tmp_path):
     ref = oracle.bf_cg(c, cg_num=3, lam=1e-2, tv=True, tv_num=2, eps=1e-6, use_z=0)
     # "%f" keeps 6 decimals
     assert np.max(np.abs(xr + 1j * xi - ref)) < 1e-5 + 1e-4 * np.max(np.abs(ref))
+
+
+def test_batch_with_uneven_trajectories(pkg, ctx, synth):
+    """imp_bruteforce_batch: slices with their own spirals of different lengths
+    and their own field maps; each slice equals the single-slice call on its own
+    trajectory and stays within 1e-4 of the FP64 oracle."""
+    from gpu_util import gpu_recon
+    rng = np.random.default_rng(17)
+    n, C = 32, 2
+    ix, iy, iz = synth.grid_positions(n, n, 1)
+    sens = np.stack([synth.to_voxel_order(m) for m in synth.coil_maps((n, n), C, rng)])
+    cases = []
+    for il in (3, 5, 4):
+        kx, ky, t = synth.spiral(il, 256, n / 2, rng)
+        img = synth.to_voxel_order(synth.ellipse_phantom((n, n), 6, rng))
+        fm = synth.to_voxel_order(synth.field_map((n, n), rng)).astype(np.float32)
+        c = dict(kx=kx, ky=ky, kz=np.zeros_like(kx), t=t, ix=ix, iy=iy, iz=iz, fm=fm,
+                 sens=sens.astype(np.complex64), dims=(n, n, 1), opts=dict(use_z=0))
+        c["kdata"] = synth.add_noise(oracle.ft(img, c, use_z=0), 40.0, rng).astype(np.complex64)
+        cases.append(c)
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    k_off = np.cumsum([0] + [c["kx"].size for c in cases])
+    cat = lambda k: f32(np.concatenate([c[k] for c in cases]))
+    kd = np.concatenate([np.asarray(c["kdata"]).ravel() for c in cases])
+    N = n * n
+    xr = np.zeros(3 * N, np.float32)
+    xi = np.zeros(3 * N, np.float32)
+    opts = pkg.bf_options(cg_num=4, fd_penalizer=1e-2, tv=True, tv_num=2)
+    pkg.bruteForceBatch(ctx, opts, xr, xi, f32(kd.real), f32(kd.imag), cat("kx"), cat("ky"),
+                        cat("kz"), cat("t"), k_off, ix, iy, iz, cat("fm"), f32(sens.real),
+                        f32(sens.imag), N, C)
+    for s, c in enumerate(cases):
+        got = xr[s * N:(s + 1) * N] + 1j * xi[s * N:(s + 1) * N].astype(np.float64)
+        single = gpu_recon(pkg, ctx, c, cg_num=4, lam=1e-2, tv=True, tv_num=2)
+        ref = oracle.bf_cg(c, cg_num=4, lam=1e-2, tv=True, tv_num=2, eps=1e-6, use_z=0)
+        assert oracle.rel_l2(got, single) < 1e-6
+        assert oracle.rel_l2(got, ref) < TOL_IMG

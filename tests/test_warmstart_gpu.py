@@ -1,6 +1,6 @@
 """What the trained network gains over plain CG, at a small scale that trains
-in seconds: 64x64 images, 4 coils, an 8 x 512 spiral, 96 training phantoms
-with 50-iteration CG labels.  The network's starting image must be much closer
+in seconds: 64x64 images, 4 coils, an 8 x 512 spiral, 320 training phantoms
+with 50-iteration CG labels (regularized CG: lambda = 1e-3 lambda_max).  The network's starting image must be much closer
 to the converged solution than zero, and CG from it must need fewer updates to
 reach NRMSE 1e-3 against the converged solution than CG from zero.  Plus the
 warm-start CG entry
@@ -80,14 +80,14 @@ def test_cg_after_a_tolerance_stop_starts_clean(pkg, ctx, prob):
 def test_network_warm_start_saves_iterations(pkg, ctx, prob):
     import torch
     from impatient_mri_b200 import learn
-    b, lab, _ = prob.make_pairs(112, seed=5)
-    x, y, kappa = learn.normalise(b[:96], lab[:96])
+    b, lab, _ = prob.make_pairs(328, seed=5)
+    x, y, kappa = learn.normalise(b[:320], lab[:320])
     net = pkg.UNet(ctx, 8, 64, 64, seed=7)
     net1 = pkg.UNet(ctx, 1, 64, 64, seed=7)
     try:
-        losses = learn.train(net, x, y, epochs=40, lr=2e-3)
+        losses = learn.train(net, x, y, epochs=60, lr=2e-3)
         net1.set_params(net.get_params())
-        res = learn.evaluate(prob, net1, kappa, b[96:104], target=1e-3, kmax=600)
+        res = learn.evaluate(prob, net1, kappa, b[320:328], target=1e-3, kmax=300)
     finally:
         net.close()
         net1.close()
@@ -100,5 +100,5 @@ def test_network_warm_start_saves_iterations(pkg, ctx, prob):
           f"CG updates to NRMSE 1e-3: zero {it_z:.1f}, warm {it_w:.1f}; "
           f"to relative residual 1e-4: zero {it_tz:.1f}, warm {it_tw:.1f}")
     assert losses[-1] < 0.5 * losses[0]
-    assert x0 < 0.5
+    assert x0 < 0.3
     assert it_w < it_z
