@@ -17,7 +17,7 @@ the given SNR, gridded by the F^H d path) and the label is the plain
 50-iteration zero-start CG solution.  The U-Net maps b / rms(b) to
 label / (rms(b) kappa); kappa is the median label-to-input RMS ratio of the
 training set.  At test time the network output, rescaled, is the CG's
-starting image; plain zero-start CG is the fallback and the judge of its error.
+starting image; plain zero-start CG is the fallback and the reference for its error.
 """
 from __future__ import annotations
 
