@@ -734,6 +734,110 @@ def run_batch(args, local):
     return 0
 
 
+def run_toeplitz_ref_gpu(args):
+    """The reference's own GPU program (oracle/_ref/mriSolver_ref, built from the
+    reference sources by oracle/build_ref_gpu.sh) against this build's mriSolver
+    on the same input directory and flags (the Toeplitz configuration, written
+    in the 1.0 format): wall time of each whole program run, file I/O included,
+    and the reference's own printed kernel times."""
+    import re
+    import tempfile
+    from __graft_entry__ import load_package
+    load_package()
+    from impatient_mri_b200 import io as mio, synth
+    ref = ROOT / "oracle" / "_ref" / "mriSolver_ref"
+    ours = ROOT / "impatient-mri_b200" / "bin" / "mriSolver"
+    if not ref.exists():
+        print(json.dumps({"impl": "reference-gpu", "unavailable":
+                          "oracle/_ref/mriSolver_ref not built (oracle/build_ref_gpu.sh)"}))
+        return 0
+    case = synth.make_case(TOEP, seed=1003)
+    o = case["opts"]
+    M, N, C = case["M"], case["N"], case["num_coil"]
+    rng = np.random.default_rng(11)
+    kd = ((rng.standard_normal((C, M)) + 1j * rng.standard_normal((C, M)))
+          * np.sqrt(np.mean(np.abs(case["x_true"]) ** 2) * N / 2)).astype(np.complex64)
+    flags = ["-toeplitzGridding", "-ntime_segs", str(o["ntime_segs"]), "-gridOS_Q",
+             str(o["gridOS_Q"]), "-gridOS_FH", str(o["gridOS_FH"]), "-cg_num",
+             str(args.ref_cg), "-fdp", str(o["fd_penalizer"])]
+    if args.ref_tv:
+        flags += ["-tv", "-tv_num", str(o["tv_num"])]
+    out = {"impl": "reference-gpu", "workload": TOEP, "flags": " ".join(flags)}
+    with tempfile.TemporaryDirectory() as d:
+        mio.write_dataset(d, "1.0", kx=case["kx"], ky=case["ky"], kz=case["kz"], t=case["t"],
+                          ix=case["ix"], iy=case["iy"], iz=case["iz"], fm=case["fm"], kdata=kd,
+                          sensi=case["sens"], dims=case["dims"], num_coil=C)
+        for name, exe in (("ours", ours), ("reference", ref)):
+            t0 = time.perf_counter()
+            try:
+                r = subprocess.run([str(exe), "-idir", d, *flags], capture_output=True,
+                                   text=True, timeout=args.ref_timeout)
+                wall = time.perf_counter() - t0
+                res = {"wall_s": wall, "rc": r.returncode}
+                for key, pat in (("q_ms", r"Q Kernel Time: ([0-9.]+)"),
+                                 ("fhd_ms", r"F\^H\(d\) Kernel Time: ([0-9.]+)"),
+                                 ("cg_ms", r"CG Execution Time: ([0-9.]+)")):
+                    mt = re.search(pat, r.stdout)
+                    if mt:
+                        res[key] = float(mt.group(1))
+                if r.returncode != 0:
+                    res["tail"] = (r.stdout + r.stderr)[-400:]
+            except subprocess.TimeoutExpired:
+                res = {"wall_s": None, "timeout_s": args.ref_timeout}
+            out[name] = res
+            print(f"{name}: {res}", file=sys.stderr, flush=True)
+    print(json.dumps(out))
+    return 0
+
+
+def run_unet_only(args, local):
+    """Training steps of the warm start's U-Net at 512x512, batch 8 (the small
+    command the U-Net kernel profiles are taken on), timed with CUDA events.
+    FLOP = 2 MACs forward + 4 MACs backward per image (data and weight
+    gradients), against the measured dense BF16 tensor peak."""
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from impatient_mri_b200 import learn
+    torch.cuda.set_device(local)
+    B, H, W = args.batch, 512, 512
+    g = torch.Generator(device="cuda").manual_seed(3)
+    x = torch.randn(B, 2, H * W, device="cuda", generator=g)
+    t = 0.5 * x
+    with pkg.Context(local) as ctx:
+        net = pkg.UNet(ctx, B, H, W, seed=1)
+        for _ in range(max(args.warmup, 1)):
+            net.train_step(x, t, 1e-4)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            net.train_step(x, t, 1e-4)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / max(args.steps, 1)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        y = torch.zeros_like(x)
+        f0.record()
+        for _ in range(args.steps):
+            net.forward(x, y)
+        f1.record()
+        torch.cuda.synchronize()
+        ms_f = f0.elapsed_time(f1) / max(args.steps, 1)
+        net.close()
+    macs = learn.unet_macs(H, W) * B
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (
+        ROOT / "MEASURED_PEAKS.json").exists() else {}
+    bf16 = float(peaks.get("bf16_tflops", 1590.0))
+    tf_train = 6.0 * macs / (ms / 1e3) / 1e12
+    tf_fwd = 2.0 * macs / (ms_f / 1e3) / 1e12
+    print(json.dumps({"unet_only": f"512x512 batch {B}", "ms_per_train_step": ms,
+                      "ms_per_forward": ms_f, "train_tflops": tf_train, "forward_tflops": tf_fwd,
+                      "bf16_peak_tflops": bf16, "forward_frac": tf_fwd / bf16,
+                      "train_frac": tf_train / bf16}))
+    return 0
+
+
 def run_nudft_only(args, local):
     """Forward + adjoint NUDFT applies of the benchmark geometry through the
     operator C-ABI (the small command the kernel profiles are taken on)."""
@@ -766,12 +870,17 @@ def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--nudft-only", action="store_true",
                     help="only forward + adjoint NUDFT applies (profiling command)")
+    ap.add_argument("--unet-only", action="store_true",
+                    help="only U-Net training steps at 512x512 (profiling command)")
     ap.add_argument("--toep-apply-only", action="store_true",
                     help="only Toeplitz A^H A applications (profiling command)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
+    ap.add_argument("--ref-cg", type=int, default=20, help="reference-gpu: cg_num")
+    ap.add_argument("--ref-tv", action="store_true", help="reference-gpu: add -tv -tv_num 10")
+    ap.add_argument("--ref-timeout", type=int, default=1200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--slices", type=int, default=4, help="batch384: slices timed")
     ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, TOEP, WARM, BATCH],
@@ -791,6 +900,10 @@ def main() -> int:
             return run_nudft_only(args, local)
         if args.toep_apply_only:
             return run_toep_apply_only(args, local)
+        if args.unet_only:
+            return run_unet_only(args, local)
+        if args.impl == "reference-gpu":
+            return run_toeplitz_ref_gpu(args) if rank == 0 else 0
         if args.impl == "reference":
             return run_reference(args, ws, rank)
         if args.workload == TOEP:

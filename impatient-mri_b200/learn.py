@@ -28,6 +28,20 @@ import numpy as np
 from . import synth
 
 
+# (cin, cout, kernel size, pyramid level) of the network's 18 convolutions,
+# in the order of the CUDA layer table (level l runs at H/2^l x W/2^l)
+UNET_LAYERS = [(16, 32, 3, 0), (32, 32, 3, 0), (32, 64, 3, 1), (64, 64, 3, 1), (64, 128, 3, 2),
+               (128, 128, 3, 2), (128, 256, 3, 3), (256, 256, 3, 3), (256, 128, 1, 3),
+               (256, 128, 3, 2), (128, 128, 3, 2), (128, 64, 1, 2), (128, 64, 3, 1),
+               (64, 64, 3, 1), (64, 32, 1, 1), (64, 32, 3, 0), (32, 32, 3, 0), (32, 16, 1, 0)]
+
+
+def unet_macs(H: int, W: int) -> int:
+    """Multiply-accumulates of one forward pass of one image (as computed,
+    padded channels included)."""
+    return sum((H >> l) * (W >> l) * co * k * k * ci for ci, co, k, l in UNET_LAYERS)
+
+
 def _torch():
     import torch
     return torch
