@@ -790,6 +790,46 @@ def run_toeplitz_ref_gpu(args):
     return 0
 
 
+def run_toep_grid_only(args, local):
+    """Q and F^H d by gridding for the Toeplitz 3-D geometry (the small command
+    the gridding profiles are taken on), timed with CUDA events."""
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from impatient_mri_b200 import synth
+    torch.cuda.set_device(local)
+    case = synth.make_case(TOEP, seed=1003)
+    o = case["opts"]
+    M, N, C = case["M"], case["N"], case["num_coil"]
+    nx, ny, nz = case["dims"]
+    L1, G = o["ntime_segs"] + 1, 8 * N
+    f = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32)).cuda()
+    rng = np.random.default_rng(11)
+    kd = (rng.standard_normal((C, M)) + 1j * rng.standard_normal((C, M))).astype(np.complex64)
+    D = {k: f(case[k]) for k in ("kx", "ky", "kz", "t", "fm")}
+    sr, si = f(case["sens"].real.ravel()), f(case["sens"].imag.ravel())
+    yr, yi = f(kd.real.ravel()), f(kd.imag.ravel())
+    qr, qi = torch.zeros(L1 * G, device="cuda"), torch.zeros(L1 * G, device="cuda")
+    fr, fi = torch.zeros(N, device="cuda"), torch.zeros(N, device="cuda")
+    opts = pkg.toeplitz_options(ntime_segs=o["ntime_segs"], gridOS_Q=o["gridOS_Q"],
+                                gridOS_FH=o["gridOS_FH"])
+    with pkg.Context(local) as ctx:
+        def run():
+            pkg.toeplitz_q(ctx, opts, qr, qi, D["kx"], D["ky"], D["kz"], D["t"], M, nx, ny, nz)
+            pkg.toeplitz_fhd(ctx, opts, fr, fi, yr, yi, D["kx"], D["ky"], D["kz"], D["t"],
+                             D["fm"], sr, si, M, C, nx, ny, nz)
+        for _ in range(max(args.warmup, 1)):
+            run()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            run()
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    print(json.dumps({"toep_grid_only": TOEP, "ms_q_plus_fhd": dt * 1e3}))
+    return 0
+
+
 def run_unet_only(args, local):
     """Training steps of the warm start's U-Net at 512x512, batch 8 (the small
     command the U-Net kernel profiles are taken on), timed with CUDA events.
@@ -870,6 +910,8 @@ def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--nudft-only", action="store_true",
                     help="only forward + adjoint NUDFT applies (profiling command)")
+    ap.add_argument("--toep-grid-only", action="store_true",
+                    help="only Toeplitz Q and F^H d gridding (profiling command)")
     ap.add_argument("--unet-only", action="store_true",
                     help="only U-Net training steps at 512x512 (profiling command)")
     ap.add_argument("--toep-apply-only", action="store_true",
@@ -902,6 +944,8 @@ def main() -> int:
             return run_toep_apply_only(args, local)
         if args.unet_only:
             return run_unet_only(args, local)
+        if args.toep_grid_only:
+            return run_toep_grid_only(args, local)
         if args.impl == "reference-gpu":
             return run_toeplitz_ref_gpu(args) if rank == 0 else 0
         if args.impl == "reference":
