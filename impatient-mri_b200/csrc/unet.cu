@@ -4,14 +4,19 @@
 // accumulation): forward and data-gradient share one kernel (the data
 // gradient is the forward conv of the masked output gradient with flipped,
 // transposed weights); the weight gradient is a split-K GEMM over pixels.
-// Tiles are staged with cp.async double buffering.
+// The convolution runs on tcgen05 (TMA-fed stages, accumulator in tensor
+// memory); a WMMA kernel with cp.async double buffering is kept as the
+// alternative selected by IMP_UNET_WMMA=1.
 #include "common.cuh"
 #include "unet.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <mma.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <random>
 #include <vector>
 
@@ -19,6 +24,19 @@ namespace imp {
 
 using bf16 = __nv_bfloat16;
 using namespace nvcuda;
+
+// Arguments of one convolution launch (forward or data gradient).
+struct ConvArgs {
+    const bf16 *x;
+    int ldx, xoff;          // input channel stride and offset
+    const bf16 *w;          // [cout][ks*ks*cin]
+    const float *bias;      // [cout] or null
+    bf16 *y;                // BF16 output or null
+    int ldy, yoff;
+    float *yf;              // FP32 output or null
+    int ldyf, yfoff, accumulate;
+    int B, H, W, cin, cout, ks, relu;
+};
 
 namespace {
 
@@ -38,17 +56,7 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-struct ConvArgs {
-    const bf16 *x;
-    int ldx, xoff;          // input channel stride and offset
-    const bf16 *w;          // [cout][ks*ks*cin]
-    const float *bias;      // [cout] or null
-    bf16 *y;                // BF16 output or null
-    int ldy, yoff;
-    float *yf;              // FP32 output or null
-    int ldyf, yfoff, accumulate;
-    int B, H, W, cin, cout, ks, relu;
-};
+
 
 // out[p][co] = act(bias + sum_{tap, ci} in[p + shift(tap)][ci] w[co][tap][ci]),
 // zero padding; 64 pixels x 64 output channels per block.
@@ -421,6 +429,331 @@ __global__ void k_to_bf16(bf16 *o, const float *s, size_t n) {
         o[i] = __float2bfloat16(s[i]);
 }
 
+// ---------------------------------------------------------------------------
+// tcgen05 implicit-GEMM convolution (sm_100a).  One block computes a patch of
+// 8 x 16 pixels of one image (M = 128 GEMM rows) times NT output channels
+// (N), K = taps x input channels in chunks of CK channels.  Per K step the
+// TMA warp loads the patch shifted by the tap, {CK, 16, 8, 1} of the NHWC
+// activations (coordinates outside the image read zeros: the convolution's
+// padding), and the {CK, NT} slice of the weights into one of S stages; the
+// MMA warp issues CK/16 tcgen05.mma into the FP32 accumulator in tensor
+// memory and releases the stage through tcgen05.commit; the four epilogue
+// warps read the accumulator with tcgen05.ld and store BF16 / FP32 rows with
+// bias and ReLU fused.  Every mbarrier wait is bounded.
+// Both operands are K-major with the TMA swizzle whose span is one row of the
+// tile (CK * 2 bytes: 32, 64 or 128 B), i.e. 8-row atoms of CK * 16 bytes,
+// which is the UMMA canonical K-major swizzled layout (leading byte offset
+// unused = 1, stride byte offset = one atom).
+// ---------------------------------------------------------------------------
+constexpr int kTcM = 128;
+constexpr int kTcThreads = 192;  // warps 0-3 epilogue, warp 4 TMA, warp 5 MMA
+constexpr int kTileX = 16, kTileY = 8;
+
+// Shared-memory matrix descriptor (version 1): start address, leading byte
+// offset 16 B, stride byte offset sbo, swizzle layout code (2 = 128 B,
+// 4 = 64 B, 6 = 32 B).
+__device__ __forceinline__ uint64_t umma_desc_sw(unsigned saddr, unsigned sbo, unsigned layout) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)layout << 61;
+    return d;
+}
+
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, int c0, int c1,
+                                            int c2, int c3, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
+        "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, int c0, int c1,
+                                            uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Instruction descriptor: BF16 x BF16 -> F32, A and B K-major, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait_tc(uint64_t *bar, unsigned parity) {
+    for (unsigned it = 0; it < (1u << 22); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// Pipeline depth for a stage of `stage` bytes: about 96 KB of stages, so two
+// blocks share an SM (one's epilogue overlaps the other's main loop).
+__host__ __device__ constexpr int tc_stages(int stage) {
+    return (96 * 1024) / stage < 2 ? 2 : ((96 * 1024) / stage > 8 ? 8 : (96 * 1024) / stage);
+}
+
+template <int CK, int NT>
+__global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ CUtensorMap tmx,
+                                                         const __grid_constant__ CUtensorMap tmw,
+                                                         ConvArgs a, int tiles_x, int tiles_y,
+                                                         unsigned *err) {
+    constexpr int A_BYTES = kTcM * CK * 2;
+    constexpr int B_REAL = NT * CK * 2;
+    constexpr int B_BYTES = (B_REAL + 1023) / 1024 * 1024;
+    constexpr int STAGE = A_BYTES + B_BYTES;
+    constexpr int S = tc_stages(STAGE);
+    constexpr int TCOLS = NT < 32 ? 32 : NT;
+    constexpr uint32_t IDESC = umma_idesc_bf16(kTcM, NT);
+    constexpr unsigned LAYOUT = CK == 64 ? 2u : (CK == 32 ? 4u : 6u);
+    constexpr unsigned SBO = 8 * CK * 2;
+    extern __shared__ unsigned char smraw[];
+    __shared__ __align__(8) uint64_t full[S], empty[S], done;
+    __shared__ uint32_t tmem_sh;
+    // Stage tiles start on 1024-byte boundaries (the swizzle pattern's period).
+    unsigned char *sm = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int t = blockIdx.x;
+    const int x0 = (t % tiles_x) * kTileX;
+    t /= tiles_x;
+    const int y0 = (t % tiles_y) * kTileY;
+    const int b = t / tiles_y;
+    const int n0 = blockIdx.y * NT;
+    const int cpt = a.cin / CK;  // channel chunks per tap
+    const int nk = a.ks * a.ks * cpt;
+    const int half = a.ks / 2;
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_sh)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 4 && lane == 0) {
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmx)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmw)) : "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_sh;
+
+    if (warp == 4) {
+        if (lane == 0) {  // TMA producer
+            bool ok = true;
+            for (int k = 0; k < nk; ++k) {
+                const int s = k % S;
+                const unsigned u = (unsigned)(k / S);
+                if (k >= S && !mbar_wait_tc(&empty[s], (u - 1) & 1)) ok = false;
+                const int tap = k / cpt, c0 = (k - tap * cpt) * CK;
+                const int dy = tap / a.ks - half, dx = tap % a.ks - half;
+                unsigned char *sa = sm + s * STAGE;
+                mbar_arrive_expect_tx(&full[s], A_BYTES + B_REAL);
+                tma_load_4d(sa, &tmx, c0, x0 + dx, y0 + dy, b, &full[s]);
+                tma_load_2d(sa + A_BYTES, &tmw, tap * a.cin + c0, n0, &full[s]);
+            }
+            if (!ok && err) atomicOr(err, DEV_ERR_TIMEOUT);
+        }
+        __syncwarp();
+    } else if (warp == 5) {
+        if (lane == 0) {  // MMA issuer
+            bool ok = true;
+            for (int k = 0; k < nk; ++k) {
+                const int s = k % S;
+                const unsigned u = (unsigned)(k / S);
+                if (!mbar_wait_tc(&full[s], u & 1)) ok = false;
+                tc_fence_after();
+                const unsigned sa = smem_u32(sm + s * STAGE);
+                const unsigned sb = sa + A_BYTES;
+#pragma unroll
+                for (int kk = 0; kk < CK / 16; ++kk) {
+                    const uint64_t da = umma_desc_sw(sa + kk * 32, SBO, LAYOUT);
+                    const uint64_t db = umma_desc_sw(sb + kk * 32, SBO, LAYOUT);
+                    const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
+                            tmem),
+                        "l"(da), "l"(db), "r"(IDESC), "r"(acc)
+                        : "memory");
+                }
+                asm volatile(
+                    "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 "
+                    "[%0];" ::"r"(smem_u32(&empty[s]))
+                    : "memory");
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    smem_u32(&done))
+                : "memory");
+            if (!ok && err) atomicOr(err, DEV_ERR_TIMEOUT);
+        }
+        __syncwarp();
+    } else {  // epilogue: warp w reads accumulator lanes (rows) 32w .. 32w + 31
+        if (!mbar_wait_tc(&done, 0)) {
+            if (err && lane == 0) atomicOr(err, DEV_ERR_TIMEOUT);
+            mbar_wait_tc(&done, 0);  // once more, bounded
+        }
+        tc_fence_after();
+        const int r = warp * 32 + lane;
+        const int xx = x0 + (r & (kTileX - 1)), yy = y0 + r / kTileX;
+        const bool valid = xx < a.W && yy < a.H;
+        const size_t p = ((size_t)b * a.H + yy) * a.W + xx;
+#pragma unroll 1
+        for (int c0 = 0; c0 < NT; c0 += 16) {
+            uint32_t v[16];
+            __syncwarp();
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+                "%12,%13,%14,%15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                  "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                  "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            const int co = n0 + c0;
+            if (!valid || co >= a.cout) continue;
+            float f[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                f[j] = __uint_as_float(v[j]);
+                if (a.bias) f[j] += a.bias[co + j];
+                if (a.relu) f[j] = fmaxf(f[j], 0.f);
+            }
+            if (a.y) {
+                uint4 q[2];
+                uint32_t *qw = reinterpret_cast<uint32_t *>(q);
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const __nv_bfloat162 h = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+                    qw[j] = *reinterpret_cast<const uint32_t *>(&h);
+                }
+                uint4 *d = reinterpret_cast<uint4 *>(a.y + p * a.ldy + a.yoff + co);
+                d[0] = q[0];
+                d[1] = q[1];
+            }
+            if (a.yf) {
+                float4 *d = reinterpret_cast<float4 *>(a.yf + p * a.ldyf + a.yfoff + co);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float4 o = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+                    if (a.accumulate) {
+                        const float4 g = d[j];
+                        o.x += g.x;
+                        o.y += g.y;
+                        o.z += g.z;
+                        o.w += g.w;
+                    }
+                    d[j] = o;
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 5)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TCOLS)
+                     : "memory");
+}
+
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime
+// (no link-time dependency on libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+template <int CK, int NT>
+cudaError_t launch_conv_tc(const ConvArgs &a, unsigned *err, cudaStream_t st) {
+    constexpr int STAGE = kTcM * CK * 2 + (NT * CK * 2 + 1023) / 1024 * 1024;
+    constexpr int SMEM = tc_stages(STAGE) * STAGE + 1024;
+    const auto enc = tmap_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    cudaError_t e = cudaFuncSetAttribute(k_conv_tc<CK, NT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    if (e != cudaSuccess) return e;
+    const CUtensorMapSwizzle swz = CK == 64 ? CU_TENSOR_MAP_SWIZZLE_128B
+                                   : CK == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                              : CU_TENSOR_MAP_SWIZZLE_32B;
+    // Activations: {channel, x, y, image} of the channel slice [xoff, xoff + cin).
+    CUtensorMap tmx, tmw;
+    const cuuint64_t xd[4] = {(cuuint64_t)a.cin, (cuuint64_t)a.W, (cuuint64_t)a.H,
+                              (cuuint64_t)a.B};
+    const cuuint64_t xs[3] = {(cuuint64_t)a.ldx * 2, (cuuint64_t)a.ldx * 2 * a.W,
+                              (cuuint64_t)a.ldx * 2 * a.W * a.H};
+    const cuuint32_t xb[4] = {(cuuint32_t)CK, kTileX, kTileY, 1};
+    const cuuint32_t one[4] = {1, 1, 1, 1};
+    if (enc(&tmx, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)(a.x + a.xoff), xd, xs, xb, one,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
+    // Weights: {k, output channel}, k = tap * cin + input channel.
+    const int K = a.ks * a.ks * a.cin;
+    const cuuint64_t wd[2] = {(cuuint64_t)K, (cuuint64_t)a.cout};
+    const cuuint64_t ws[1] = {(cuuint64_t)K * 2};
+    const cuuint32_t wb[2] = {(cuuint32_t)CK, (cuuint32_t)NT};
+    if (enc(&tmw, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)a.w, wd, ws, wb, one,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
+    const int tiles_x = (a.W + kTileX - 1) / kTileX, tiles_y = (a.H + kTileY - 1) / kTileY;
+    const dim3 grid((unsigned)(tiles_x * tiles_y * a.B), (unsigned)((a.cout + NT - 1) / NT));
+    k_conv_tc<CK, NT><<<grid, kTcThreads, SMEM, st>>>(tmx, tmw, a, tiles_x, tiles_y, err);
+    return cudaGetLastError();
+}
+
+template <int CK>
+cudaError_t conv_tc_n(const ConvArgs &a, unsigned *err, cudaStream_t st) {
+    if (a.cout <= 16) return launch_conv_tc<CK, 16>(a, err, st);
+    if (a.cout <= 32) return launch_conv_tc<CK, 32>(a, err, st);
+    if (a.cout <= 64) return launch_conv_tc<CK, 64>(a, err, st);
+    return launch_conv_tc<CK, 128>(a, err, st);
+}
+
+// The tensor-memory path for a convolution: channel counts multiples of 16,
+// channel strides and offsets multiples of 16 (16-byte aligned TMA rows and
+// vector stores).
+cudaError_t conv_tc(const ConvArgs &a, int, unsigned *err, cudaStream_t st) {
+    if (a.cin % 16 || a.cout % 16 || a.ldx % 16 || a.xoff % 16 || a.xoff + a.cin > a.ldx ||
+        (a.y && (a.ldy % 16 || a.yoff % 16 || a.yoff + a.cout > a.ldy)) ||
+        (a.yf && (a.ldyf % 16 || a.yfoff % 16 || a.yfoff + a.cout > a.ldyf)) ||
+        (a.ks != 1 && a.ks != 3) || a.B < 1 || a.H < 1 || a.W < 1)
+        return cudaErrorInvalidValue;
+    if (a.cin % 64 == 0) return conv_tc_n<64>(a, err, st);
+    if (a.cin % 32 == 0) return conv_tc_n<32>(a, err, st);
+    return conv_tc_n<16>(a, err, st);
+}
+
 int gridn_u(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 32); }
 
 constexpr int kLossBlocks = 296;
@@ -457,9 +790,13 @@ enum {
     A_F3B, A_T2, A_F2A, A_F2B, A_T1, A_F1A, A_F1B, A_OUT, A_COUNT
 };
 
-cudaError_t UNet::setup(int batch, int H, int W, unsigned long long seed, cudaStream_t st) {
+cudaError_t UNet::setup(int batch, int H, int W, unsigned long long seed, cudaStream_t st,
+                        unsigned *err) {
     release();
     st_ = st;
+    err_ = err;
+    const char *wm = std::getenv("IMP_UNET_WMMA");
+    use_tc_ = !(wm && wm[0] == '1');
     B_ = batch;
     H_ = H;
     W_ = W;
@@ -580,12 +917,18 @@ cudaError_t UNet::conv_fwd(int li, const Act &in, int in_off, Act &out, int out_
         a.yoff = out_off;
     }
     const int P = B_ * in.H * in.W;
-    const dim3 grid((P + 63) / 64, (L.cout + 63) / 64);
-    if (L.cin % 32 == 0)
+    return run_conv(a, P);
+}
+
+// Tensor-memory (tcgen05) kernel unless IMP_UNET_WMMA=1 selects the WMMA one.
+cudaError_t UNet::run_conv(const ConvArgs &a, int P) {
+    ++launches_;
+    if (use_tc_) return conv_tc(a, P, err_, st_);
+    const dim3 grid((P + 63) / 64, (a.cout + 63) / 64);
+    if (a.cin % 32 == 0)
         k_conv_fwd<32><<<grid, kCT, 0, st_>>>(a);
     else
         k_conv_fwd<16><<<grid, kCT, 0, st_>>>(a);
-    ++launches_;
     return cudaGetLastError();
 }
 
@@ -635,12 +978,8 @@ cudaError_t UNet::conv_bwd(int li, Act &in, int in_off, Act &out, int out_off) {
         a.cout = L.cin;
         a.ks = L.ks;
         a.relu = 0;
-        const dim3 grid((P + 63) / 64, (L.cin + 63) / 64);
-        if (L.cout % 32 == 0)
-            k_conv_fwd<32><<<grid, kCT, 0, st_>>>(a);
-        else
-            k_conv_fwd<16><<<grid, kCT, 0, st_>>>(a);
-        ++launches_;
+        cudaError_t e = run_conv(a, P);
+        if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
 }
@@ -810,7 +1149,7 @@ imp_status imp_unet_create(imp_context *ctx, int batch, int height, int width,
     if (s != IMP_OK) return s;
     imp_unet *u = new imp_unet();
     u->ctx = ctx;
-    cudaError_t e = u->net.setup(batch, height, width, seed, ctx->stream);
+    cudaError_t e = u->net.setup(batch, height, width, seed, ctx->stream, ctx->dev_err);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
         delete u;

@@ -19,6 +19,8 @@
 
 namespace imp {
 
+struct ConvArgs;
+
 struct ConvLayer {
     int cin = 0, cout = 0, ks = 3;
     bool relu = true;
@@ -34,7 +36,8 @@ public:
     UNet &operator=(const UNet &) = delete;
 
     // Batch, image size (H, W multiples of 8), seed for the He initialisation.
-    cudaError_t setup(int batch, int H, int W, unsigned long long seed, cudaStream_t st);
+    cudaError_t setup(int batch, int H, int W, unsigned long long seed, cudaStream_t st,
+                      unsigned *err);
     // x: [B][2][H*W] FP32 (channel-major per image), y: same; the network
     // output for channels 0 and 1.
     cudaError_t forward(const float *x, float *y);
@@ -67,6 +70,7 @@ private:
     cudaError_t conv_fwd(int li, const Act &in, int in_off, Act &out, int out_off);
     cudaError_t conv_bwd(int li, Act &in, int in_off, Act &out, int out_off);
     cudaError_t pack_input(const float *x);
+    cudaError_t run_conv(const ConvArgs &a, int P);
     cudaError_t run_forward();
 
     cudaStream_t st_ = nullptr;
@@ -84,6 +88,8 @@ private:
     std::vector<Act> acts_;
     int step_ = 0;
     long launches_ = 0;
+    unsigned *err_ = nullptr;  // device error word (bounded-wait timeouts)
+    bool use_tc_ = true;       // tcgen05 convolutions (else WMMA)
 };
 
 }  // namespace imp

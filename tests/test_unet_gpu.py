@@ -96,3 +96,25 @@ def test_training_reduces_loss(pkg, ctx):
         net.close()
     print(f"loss {losses[0]:.4f} -> {losses[-1]:.4f}")
     assert losses[-1] < 0.2 * losses[0]
+
+
+def test_tensor_memory_and_wmma_kernels_agree(pkg, ctx, monkeypatch):
+    """The tcgen05 convolution (accumulator in tensor memory) and the WMMA one
+    give the same forward pass and gradients up to FP32 summation order."""
+    B, H, W = 2, 32, 32
+    x, t = data(B, H, W, 5)
+    nets = {}
+    for name, env in (("tc", "0"), ("wmma", "1")):
+        monkeypatch.setenv("IMP_UNET_WMMA", env)
+        net = pkg.UNet(ctx, B, H, W, seed=21)
+        try:
+            y = net.forward(x, np.zeros_like(x))
+            loss, g = net.gradients(x, t)
+        finally:
+            net.close()
+        nets[name] = (y, loss, g)
+    (y1, l1, g1), (y2, l2, g2) = nets["tc"], nets["wmma"]
+    print(f"tc vs wmma: forward {rel(y1, y2):.2e}, gradients {rel(g1, g2):.2e}")
+    assert rel(y1, y2) < 1e-2
+    assert abs(l1 - l2) / l2 < 1e-3
+    assert rel(g1, g2) < 5e-2
