@@ -20,6 +20,12 @@
 #include <random>
 #include <vector>
 
+#define U_TRY(x)                              \
+    do {                                      \
+        cudaError_t e_ = (x);                 \
+        if (e_ != cudaSuccess) return e_;     \
+    } while (0)
+
 namespace imp {
 
 using bf16 = __nv_bfloat16;
@@ -36,6 +42,7 @@ struct ConvArgs {
     float *yf;              // FP32 output or null
     int ldyf, yfoff, accumulate;
     int B, H, W, cin, cout, ks, relu;
+    int up2;                // BF16 output written to the 2 x 2 block of an image of size 2H x 2W
 };
 
 namespace {
@@ -258,28 +265,69 @@ __global__ void __launch_bounds__(kCT) k_wgrad(WgArgs a) {
     }
 }
 
-// db[co] += sum_p dz[p][co]
-__global__ void k_bgrad(float *db, const bf16 *dz, int P, int cout) {
-    const int pb = blockIdx.x * 256;
-    const int pe = min(P, pb + 256);
-    for (int c = threadIdx.x; c < cout; c += blockDim.x) {
-        float s = 0.f;
-        for (int p = pb; p < pe; ++p) s += __bfloat162float(dz[(size_t)p * cout + c]);
-        atomicAdd(&db[c], s);
+// Eight BF16 <-> FP32 values as one 16-byte vector.
+__device__ __forceinline__ void bf16x8_to_f32(const uint4 &q, float *f) {
+    const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&q);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float2 t = __bfloat1622float2(h[j]);
+        f[2 * j] = t.x;
+        f[2 * j + 1] = t.y;
     }
 }
+__device__ __forceinline__ uint4 f32_to_bf16x8(const float *f) {
+    uint32_t w[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const __nv_bfloat162 h = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+        w[j] = ((uint32_t)__bfloat16_as_ushort(h.y) << 16) | __bfloat16_as_ushort(h.x);
+    }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
 
-// dz[p][co] = g[p][goff + co] * (relu ? (y[p][yoff + co] > 0) : 1), as BF16
+// db[co] += sum_p dz[p][co].  Thread = 8 channels x a pixel lane (cout / 8
+// divides the block); lanes are summed in shared memory, then one atomic per
+// channel and block.
+__global__ void k_bgrad(float *db, const bf16 *dz, int P, int cout) {
+    __shared__ float acc[256];
+    const int groups = cout >> 3, lanes = blockDim.x / groups;
+    const int cg = threadIdx.x % groups, pl = threadIdx.x / groups;
+    for (int c = threadIdx.x; c < cout; c += blockDim.x) acc[c] = 0.f;
+    __syncthreads();
+    float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int p = blockIdx.x * lanes + pl; p < P; p += gridDim.x * lanes) {
+        float f[8];
+        bf16x8_to_f32(*reinterpret_cast<const uint4 *>(dz + (size_t)p * cout + cg * 8), f);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s[j] += f[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) atomicAdd(&acc[cg * 8 + j], s[j]);
+    __syncthreads();
+    for (int c = threadIdx.x; c < cout; c += blockDim.x) atomicAdd(&db[c], acc[c]);
+}
+
+// dz[p][co] = g[p][goff + co] * (relu ? (y[p][yoff + co] > 0) : 1), as BF16;
+// 8 channels per thread (cout, ldg, goff, ldy, yoff multiples of 8).
 __global__ void k_dz(bf16 *dz, const float *g, int ldg, int goff, const bf16 *y, int ldy, int yoff,
                      int P, int cout, int relu) {
-    const size_t n = (size_t)P * cout;
+    const int groups = cout >> 3;
+    const size_t n = (size_t)P * groups;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
-        const size_t p = i / cout;
-        const int c = (int)(i % cout);
-        float v = g[p * ldg + goff + c];
-        if (relu && !(__bfloat162float(y[p * ldy + yoff + c]) > 0.f)) v = 0.f;
-        dz[i] = __float2bfloat16(v);
+        const size_t p = i / groups;
+        const int c = (int)(i - p * groups) * 8;
+        const float4 *gp = reinterpret_cast<const float4 *>(g + p * ldg + goff + c);
+        const float4 g0 = gp[0], g1 = gp[1];
+        float v[8] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+        if (relu) {
+            float yv[8];
+            bf16x8_to_f32(*reinterpret_cast<const uint4 *>(y + p * ldy + yoff + c), yv);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (!(yv[j] > 0.f)) v[j] = 0.f;
+        }
+        *reinterpret_cast<uint4 *>(dz + p * cout + c) = f32_to_bf16x8(v);
     }
 }
 
@@ -296,87 +344,113 @@ __global__ void k_wtrans(bf16 *wt, const bf16 *w, int cin, int cout, int taps) {
     }
 }
 
-// 2x2 max pooling; idx = argmax position (dy * 2 + dx)
+// 2x2 max pooling; idx = argmax position (dy * 2 + dx), the first of equal
+// maxima.  8 channels per thread (C, ldi, ioff multiples of 8).
 __global__ void k_pool_fwd(bf16 *out, unsigned char *idx, const bf16 *in, int ldi, int ioff, int B,
                            int H, int W, int C) {
-    const int Ho = H / 2, Wo = W / 2;
-    const size_t n = (size_t)B * Ho * Wo * C;
+    const int Ho = H / 2, Wo = W / 2, G = C >> 3;
+    const size_t n = (size_t)B * Ho * Wo * G;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        const size_t q = i / C;
+        const int c = (int)(i % G) * 8;
+        const size_t q = i / G;
         const int xo = (int)(q % Wo), yo = (int)((q / Wo) % Ho), b = (int)(q / ((size_t)Wo * Ho));
-        float best = -INFINITY;
-        int bi = 0;
+        float best[8];
+        uint32_t bi[2] = {0u, 0u};
+#pragma unroll
+        for (int j = 0; j < 8; ++j) best[j] = -INFINITY;
+#pragma unroll
         for (int d = 0; d < 4; ++d) {
             const size_t p = ((size_t)b * H + 2 * yo + (d >> 1)) * W + 2 * xo + (d & 1);
-            const float v = __bfloat162float(in[p * ldi + ioff + c]);
-            if (v > best) {
-                best = v;
-                bi = d;
-            }
+            float v[8];
+            bf16x8_to_f32(*reinterpret_cast<const uint4 *>(in + p * ldi + ioff + c), v);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                if (v[j] > best[j]) {
+                    best[j] = v[j];
+                    bi[j >> 2] = (bi[j >> 2] & ~(0xffu << (8 * (j & 3)))) | ((uint32_t)d << (8 * (j & 3)));
+                }
         }
-        out[i] = __float2bfloat16(best);
-        idx[i] = (unsigned char)bi;
+        *reinterpret_cast<uint4 *>(out + q * C + c) = f32_to_bf16x8(best);
+        *reinterpret_cast<uint2 *>(idx + q * C + c) = make_uint2(bi[0], bi[1]);
     }
 }
 
+// gin[argmax pixel][goff + c] += gout[q][c]; 4 channels per thread.
 __global__ void k_pool_bwd(float *gin, int ldg, int goff, const float *gout,
                            const unsigned char *idx, int B, int H, int W, int C) {
-    const int Ho = H / 2, Wo = W / 2;
-    const size_t n = (size_t)B * Ho * Wo * C;
+    const int Ho = H / 2, Wo = W / 2, G = C >> 2;
+    const size_t n = (size_t)B * Ho * Wo * G;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        const size_t q = i / C;
+        const int c = (int)(i % G) * 4;
+        const size_t q = i / G;
         const int xo = (int)(q % Wo), yo = (int)((q / Wo) % Ho), b = (int)(q / ((size_t)Wo * Ho));
-        const int d = idx[i];
-        const size_t p = ((size_t)b * H + 2 * yo + (d >> 1)) * W + 2 * xo + (d & 1);
-        gin[p * ldg + goff + c] += gout[i];
+        const float4 g4 = *reinterpret_cast<const float4 *>(gout + q * C + c);
+        const uint32_t id = *reinterpret_cast<const uint32_t *>(idx + q * C + c);
+        const float gv[4] = {g4.x, g4.y, g4.z, g4.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int d = (int)((id >> (8 * j)) & 3u);
+            const size_t p = ((size_t)b * H + 2 * yo + (d >> 1)) * W + 2 * xo + (d & 1);
+            gin[p * ldg + goff + c + j] += gv[j];
+        }
     }
 }
 
-// nearest x2: out[b][y][x][off + c] = in[b][y/2][x/2][c]  (H, W: output size)
+// nearest x2: out[b][y][x][off + c] = in[b][y/2][x/2][c]  (H, W: output size);
+// 8 channels per thread.
 __global__ void k_up_fwd(bf16 *out, int ldo, int ooff, const bf16 *in, int B, int H, int W,
                          int C) {
-    const size_t n = (size_t)B * H * W * C;
+    const int G = C >> 3;
+    const size_t n = (size_t)B * H * W * G;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        const size_t p = i / C;
+        const int c = (int)(i % G) * 8;
+        const size_t p = i / G;
         const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
         const size_t pi = ((size_t)b * (H / 2) + y / 2) * (W / 2) + x / 2;
-        out[p * ldo + ooff + c] = in[pi * C + c];
+        *reinterpret_cast<uint4 *>(out + p * ldo + ooff + c) =
+            *reinterpret_cast<const uint4 *>(in + pi * C + c);
     }
 }
 
-// gin[b][i][j][c] = sum of the 2 x 2 block of gout[..][goff + c]  (H, W: input size)
+// gin[b][i][j][c] += sum of the 2 x 2 block of gout[..][goff + c]  (H, W: input
+// size); 4 channels per thread.
 __global__ void k_up_bwd(float *gin, const float *gout, int ldg, int goff, int B, int H, int W,
                          int C) {
-    const size_t n = (size_t)B * H * W * C;
+    const int G = C >> 2;
+    const size_t n = (size_t)B * H * W * G;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
          i += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i % C);
-        const size_t p = i / C;
+        const int c = (int)(i % G) * 4;
+        const size_t p = i / G;
         const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
-        float s = 0.f;
+        float4 s = *reinterpret_cast<const float4 *>(gin + p * C + c);
+#pragma unroll
         for (int d = 0; d < 4; ++d) {
             const size_t po = ((size_t)b * 2 * H + 2 * y + (d >> 1)) * (2 * W) + 2 * x + (d & 1);
-            s += gout[po * ldg + goff + c];
+            const float4 v = *reinterpret_cast<const float4 *>(gout + po * ldg + goff + c);
+            s.x += v.x;
+            s.y += v.y;
+            s.z += v.z;
+            s.w += v.w;
         }
-        gin[i] += s;
+        *reinterpret_cast<float4 *>(gin + p * C + c) = s;
     }
 }
 
-// x [B][2][HW] -> X0 [P][16] (channels 2..15 zero)
+// x [B][2][HW] -> X0 [P][16] (channels 2..15 zero); one pixel per thread.
 __global__ void k_pack(bf16 *x0, const float *x, int B, int HW) {
-    const size_t n = (size_t)B * HW * 16;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-         i += (size_t)gridDim.x * blockDim.x) {
-        const int c = (int)(i & 15);
-        const size_t p = i >> 4;
+    const size_t n = (size_t)B * HW;
+    for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < n;
+         p += (size_t)gridDim.x * blockDim.x) {
         const size_t b = p / HW, r = p % HW;
-        x0[i] = __float2bfloat16(c < 2 ? x[(b * 2 + c) * HW + r] : 0.f);
+        const float f[8] = {x[(b * 2) * HW + r], x[(b * 2 + 1) * HW + r], 0.f, 0.f, 0.f, 0.f,
+                            0.f, 0.f};
+        uint4 *o = reinterpret_cast<uint4 *>(x0 + p * 16);
+        o[0] = f32_to_bf16x8(f);
+        o[1] = make_uint4(0u, 0u, 0u, 0u);
     }
 }
 
@@ -450,15 +524,26 @@ constexpr int kTcThreads = 192;  // warps 0-3 epilogue, warp 4 TMA, warp 5 MMA
 constexpr int kTileX = 16, kTileY = 8;
 
 // Shared-memory matrix descriptor (version 1): start address, leading byte
-// offset 16 B, stride byte offset sbo, swizzle layout code (2 = 128 B,
-// 4 = 64 B, 6 = 32 B).
-__device__ __forceinline__ uint64_t umma_desc_sw(unsigned saddr, unsigned sbo, unsigned layout) {
+// offset lbo, stride byte offset sbo, swizzle layout code (2 = 128 B,
+// 4 = 64 B, 6 = 32 B).  K-major swizzled operands: lbo unused (16 B), sbo =
+// one 8-row atom.  MN-major swizzled operands: lbo = distance between atom
+// columns along M / N, sbo = distance between 8-row groups along K.
+__device__ __forceinline__ uint64_t umma_desc(unsigned saddr, unsigned lbo, unsigned sbo,
+                                              unsigned layout) {
     uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
     d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
     d |= (uint64_t)1 << 46;
     d |= (uint64_t)layout << 61;
     return d;
+}
+__device__ __forceinline__ uint64_t umma_desc_sw(unsigned saddr, unsigned sbo, unsigned layout) {
+    return umma_desc(saddr, 16, sbo, layout);
+}
+
+// Swizzle layout code of a tile whose rows hold c BF16 channels (c * 2 bytes).
+__host__ __device__ constexpr unsigned sw_layout(int c) {
+    return c == 64 ? 2u : (c == 32 ? 4u : 6u);
 }
 
 __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, int c0, int c1,
@@ -469,6 +554,10 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, in
         "l"(reinterpret_cast<uint64_t>(tm)), "r"(c0), "r"(c1), "r"(c2), "r"(c3),
         "r"(smem_u32(bar))
         : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_local(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *tm, int c0, int c1,
@@ -500,11 +589,105 @@ __device__ __forceinline__ bool mbar_wait_tc(uint64_t *bar, unsigned parity) {
 }
 
 // Pipeline depth for a stage of `stage` bytes: about 96 KB of stages, so two
-// blocks share an SM (one's epilogue overlaps the other's main loop).
+// persistent blocks share an SM.
 __host__ __device__ constexpr int tc_stages(int stage) {
-    return (96 * 1024) / stage < 2 ? 2 : ((96 * 1024) / stage > 8 ? 8 : (96 * 1024) / stage);
+    return (96 * 1024) / stage < 2 ? 2 : ((96 * 1024) / stage > 12 ? 12 : (96 * 1024) / stage);
 }
 
+// Output tile t of a convolution: N tile fastest (blocks working on one pixel
+// patch at the same time share its loads in L2), then x, y, image.
+struct TcTile {
+    int x0, y0, b, n0;
+};
+__device__ __forceinline__ TcTile tc_tile(int t, int n_nt, int tiles_x, int tiles_y, int NT) {
+    TcTile r;
+    r.n0 = (t % n_nt) * NT;
+    t /= n_nt;
+    r.x0 = (t % tiles_x) * kTileX;
+    t /= tiles_x;
+    r.y0 = (t % tiles_y) * kTileY;
+    r.b = t / tiles_y;
+    return r;
+}
+
+// Epilogue of one tile for accumulator row r (pixel r of the 8 x 16 patch):
+// NT columns from tensor memory at tacc, + bias, ReLU, then 16 channels per
+// vector group to the BF16 output (at the pixel, or with up2 at the 2 x 2
+// block of the pixel in an image of twice the size: nearest up-sampling)
+// and / or the FP32 output (optionally accumulated).
+template <int NT>
+__device__ __forceinline__ void conv_tc_store(const ConvArgs &a, const TcTile &T, uint32_t tacc,
+                                              int r) {
+    const int xx = T.x0 + (r & (kTileX - 1)), yy = T.y0 + r / kTileX;
+    const bool valid = xx < a.W && yy < a.H;
+    const size_t p = ((size_t)T.b * a.H + yy) * a.W + xx;
+#pragma unroll 1
+    for (int c0 = 0; c0 < NT; c0 += 16) {
+        uint32_t v[16];
+        __syncwarp();
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+            "%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+              "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+              "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(tacc + (uint32_t)c0));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        const int co = T.n0 + c0;
+        if (!valid || co >= a.cout) continue;
+        float f[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            f[j] = __uint_as_float(v[j]);
+            if (a.bias) f[j] += a.bias[co + j];
+            if (a.relu) f[j] = fmaxf(f[j], 0.f);
+        }
+        if (a.y) {
+            uint32_t qw[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const __nv_bfloat162 h = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+                qw[j] = ((uint32_t)__bfloat16_as_ushort(h.y) << 16) | __bfloat16_as_ushort(h.x);
+            }
+            const uint4 q[2] = {make_uint4(qw[0], qw[1], qw[2], qw[3]),
+                                make_uint4(qw[4], qw[5], qw[6], qw[7])};
+            if (a.up2) {
+                const size_t W2 = 2 * (size_t)a.W;
+                const size_t p0 = ((size_t)T.b * 2 * a.H + 2 * yy) * W2 + 2 * xx;
+#pragma unroll
+                for (int d = 0; d < 4; ++d) {
+                    uint4 *o = reinterpret_cast<uint4 *>(
+                        a.y + (p0 + (d >> 1) * W2 + (d & 1)) * a.ldy + a.yoff + co);
+                    o[0] = q[0];
+                    o[1] = q[1];
+                }
+            } else {
+                uint4 *o = reinterpret_cast<uint4 *>(a.y + p * a.ldy + a.yoff + co);
+                o[0] = q[0];
+                o[1] = q[1];
+            }
+        }
+        if (a.yf) {
+            float4 *d = reinterpret_cast<float4 *>(a.yf + p * a.ldyf + a.yfoff + co);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                float4 o = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
+                if (a.accumulate) {
+                    const float4 g = d[j];
+                    o.x += g.x;
+                    o.y += g.y;
+                    o.z += g.z;
+                    o.w += g.w;
+                }
+                d[j] = o;
+            }
+        }
+    }
+}
+
+// Persistent: block i handles tiles i, i + gridDim.x, ...; the TMA warp runs
+// ahead across tile boundaries, the accumulator is double-buffered in tensor
+// memory so the epilogue of one tile overlaps the MMAs of the next.
 template <int CK, int NT>
 __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ CUtensorMap tmx,
                                                          const __grid_constant__ CUtensorMap tmw,
@@ -515,22 +698,19 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
     constexpr int B_BYTES = (B_REAL + 1023) / 1024 * 1024;
     constexpr int STAGE = A_BYTES + B_BYTES;
     constexpr int S = tc_stages(STAGE);
-    constexpr int TCOLS = NT < 32 ? 32 : NT;
+    constexpr int ACOLS = NT < 32 ? 32 : NT;  // columns of one accumulator
+    constexpr int TCOLS = 2 * ACOLS;
     constexpr uint32_t IDESC = umma_idesc_bf16(kTcM, NT);
     constexpr unsigned LAYOUT = CK == 64 ? 2u : (CK == 32 ? 4u : 6u);
     constexpr unsigned SBO = 8 * CK * 2;
     extern __shared__ unsigned char smraw[];
-    __shared__ __align__(8) uint64_t full[S], empty[S], done;
+    __shared__ __align__(8) uint64_t full[S], empty[S], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_sh;
     // Stage tiles start on 1024-byte boundaries (the swizzle pattern's period).
     unsigned char *sm = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int t = blockIdx.x;
-    const int x0 = (t % tiles_x) * kTileX;
-    t /= tiles_x;
-    const int y0 = (t % tiles_y) * kTileY;
-    const int b = t / tiles_y;
-    const int n0 = blockIdx.y * NT;
+    const int n_nt = (a.cout + NT - 1) / NT;
+    const int n_tiles = n_nt * tiles_x * tiles_y * a.B;
     const int cpt = a.cin / CK;  // channel chunks per tap
     const int nk = a.ks * a.ks * cpt;
     const int half = a.ks / 2;
@@ -546,7 +726,10 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(&done, 1);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&acc_full[i], 1);
+            mbar_init(&acc_empty[i], 4);  // one arrival per epilogue warp
+        }
         fence_mbar_init();
     }
     if (warp == 4 && lane == 0) {
@@ -561,16 +744,20 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
     if (warp == 4) {
         if (lane == 0) {  // TMA producer
             bool ok = true;
-            for (int k = 0; k < nk; ++k) {
-                const int s = k % S;
-                const unsigned u = (unsigned)(k / S);
-                if (k >= S && !mbar_wait_tc(&empty[s], (u - 1) & 1)) ok = false;
-                const int tap = k / cpt, c0 = (k - tap * cpt) * CK;
-                const int dy = tap / a.ks - half, dx = tap % a.ks - half;
-                unsigned char *sa = sm + s * STAGE;
-                mbar_arrive_expect_tx(&full[s], A_BYTES + B_REAL);
-                tma_load_4d(sa, &tmx, c0, x0 + dx, y0 + dy, b, &full[s]);
-                tma_load_2d(sa + A_BYTES, &tmw, tap * a.cin + c0, n0, &full[s]);
+            int g = 0;  // K steps issued by this block so far
+            for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+                const TcTile T = tc_tile(t, n_nt, tiles_x, tiles_y, NT);
+                for (int k = 0; k < nk; ++k, ++g) {
+                    const int s = g % S;
+                    const unsigned u = (unsigned)(g / S);
+                    if (g >= S && !mbar_wait_tc(&empty[s], (u - 1) & 1)) ok = false;
+                    const int tap = k / cpt, c0 = (k - tap * cpt) * CK;
+                    const int dy = tap / a.ks - half, dx = tap % a.ks - half;
+                    unsigned char *sa = sm + s * STAGE;
+                    mbar_arrive_expect_tx(&full[s], A_BYTES + B_REAL);
+                    tma_load_4d(sa, &tmx, c0, T.x0 + dx, T.y0 + dy, T.b, &full[s]);
+                    tma_load_2d(sa + A_BYTES, &tmw, tap * a.cin + c0, T.n0, &full[s]);
+                }
             }
             if (!ok && err) atomicOr(err, DEV_ERR_TIMEOUT);
         }
@@ -578,96 +765,65 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_tc(const __grid_constant__ 
     } else if (warp == 5) {
         if (lane == 0) {  // MMA issuer
             bool ok = true;
-            for (int k = 0; k < nk; ++k) {
-                const int s = k % S;
-                const unsigned u = (unsigned)(k / S);
-                if (!mbar_wait_tc(&full[s], u & 1)) ok = false;
+            int g = 0, it = 0;
+            for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+                const int ab = it & 1;
+                const unsigned au = (unsigned)(it >> 1);
+                // the epilogue has drained this accumulator's previous tile
+                if (it >= 2 && !mbar_wait_tc(&acc_empty[ab], (au - 1) & 1)) ok = false;
                 tc_fence_after();
-                const unsigned sa = smem_u32(sm + s * STAGE);
-                const unsigned sb = sa + A_BYTES;
+                const uint32_t dacc = tmem + (uint32_t)(ab * ACOLS);
+                for (int k = 0; k < nk; ++k, ++g) {
+                    const int s = g % S;
+                    const unsigned u = (unsigned)(g / S);
+                    if (!mbar_wait_tc(&full[s], u & 1)) ok = false;
+                    tc_fence_after();
+                    const unsigned sa = smem_u32(sm + s * STAGE);
+                    const unsigned sb = sa + A_BYTES;
 #pragma unroll
-                for (int kk = 0; kk < CK / 16; ++kk) {
-                    const uint64_t da = umma_desc_sw(sa + kk * 32, SBO, LAYOUT);
-                    const uint64_t db = umma_desc_sw(sb + kk * 32, SBO, LAYOUT);
-                    const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
+                    for (int kk = 0; kk < CK / 16; ++kk) {
+                        const uint64_t da = umma_desc_sw(sa + kk * 32, SBO, LAYOUT);
+                        const uint64_t db = umma_desc_sw(sb + kk * 32, SBO, LAYOUT);
+                        const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
+                                dacc),
+                            "l"(da), "l"(db), "r"(IDESC), "r"(acc)
+                            : "memory");
+                    }
                     asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
-                            tmem),
-                        "l"(da), "l"(db), "r"(IDESC), "r"(acc)
+                        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 "
+                        "[%0];" ::"r"(smem_u32(&empty[s]))
                         : "memory");
                 }
                 asm volatile(
                     "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 "
-                    "[%0];" ::"r"(smem_u32(&empty[s]))
+                    "[%0];" ::"r"(smem_u32(&acc_full[ab]))
                     : "memory");
             }
-            asm volatile(
-                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                    smem_u32(&done))
-                : "memory");
             if (!ok && err) atomicOr(err, DEV_ERR_TIMEOUT);
         }
         __syncwarp();
     } else {  // epilogue: warp w reads accumulator lanes (rows) 32w .. 32w + 31
-        if (!mbar_wait_tc(&done, 0)) {
-            if (err && lane == 0) atomicOr(err, DEV_ERR_TIMEOUT);
-            mbar_wait_tc(&done, 0);  // once more, bounded
-        }
-        tc_fence_after();
-        const int r = warp * 32 + lane;
-        const int xx = x0 + (r & (kTileX - 1)), yy = y0 + r / kTileX;
-        const bool valid = xx < a.W && yy < a.H;
-        const size_t p = ((size_t)b * a.H + yy) * a.W + xx;
-#pragma unroll 1
-        for (int c0 = 0; c0 < NT; c0 += 16) {
-            uint32_t v[16];
+        int it = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+            const TcTile T = tc_tile(t, n_nt, tiles_x, tiles_y, NT);
+            const int ab = it & 1;
+            const unsigned au = (unsigned)(it >> 1);
+            if (!mbar_wait_tc(&acc_full[ab], au & 1)) {
+                if (err && lane == 0) atomicOr(err, DEV_ERR_TIMEOUT);
+                mbar_wait_tc(&acc_full[ab], au & 1);  // once more, bounded
+            }
+            tc_fence_after();
+            conv_tc_store<NT>(a, T,
+                              tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(ab * ACOLS),
+                              warp * 32 + lane);
+            // this warp's rows of the accumulator are stored: release it
+            tc_fence_before();
             __syncwarp();
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
-                "%12,%13,%14,%15}, [%16];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
-                  "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
-                  "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            const int co = n0 + c0;
-            if (!valid || co >= a.cout) continue;
-            float f[16];
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                f[j] = __uint_as_float(v[j]);
-                if (a.bias) f[j] += a.bias[co + j];
-                if (a.relu) f[j] = fmaxf(f[j], 0.f);
-            }
-            if (a.y) {
-                uint4 q[2];
-                uint32_t *qw = reinterpret_cast<uint32_t *>(q);
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const __nv_bfloat162 h = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
-                    qw[j] = *reinterpret_cast<const uint32_t *>(&h);
-                }
-                uint4 *d = reinterpret_cast<uint4 *>(a.y + p * a.ldy + a.yoff + co);
-                d[0] = q[0];
-                d[1] = q[1];
-            }
-            if (a.yf) {
-                float4 *d = reinterpret_cast<float4 *>(a.yf + p * a.ldyf + a.yfoff + co);
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    float4 o = make_float4(f[4 * j], f[4 * j + 1], f[4 * j + 2], f[4 * j + 3]);
-                    if (a.accumulate) {
-                        const float4 g = d[j];
-                        o.x += g.x;
-                        o.y += g.y;
-                        o.z += g.z;
-                        o.w += g.w;
-                    }
-                    d[j] = o;
-                }
-            }
+            if (lane == 0) mbar_arrive_local(&acc_empty[ab]);
         }
     }
     tc_fence_before();
@@ -727,7 +883,13 @@ cudaError_t launch_conv_tc(const ConvArgs &a, unsigned *err, cudaStream_t st) {
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return cudaErrorInvalidValue;
     const int tiles_x = (a.W + kTileX - 1) / kTileX, tiles_y = (a.H + kTileY - 1) / kTileY;
-    const dim3 grid((unsigned)(tiles_x * tiles_y * a.B), (unsigned)((a.cout + NT - 1) / NT));
+    const long long n_tiles = (long long)tiles_x * tiles_y * a.B * ((a.cout + NT - 1) / NT);
+    if (n_tiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return cudaErrorInvalidDevice;
+    const int grid = (int)std::min<long long>(n_tiles, 2LL * sms);  // two blocks per SM
     k_conv_tc<CK, NT><<<grid, kTcThreads, SMEM, st>>>(tmx, tmw, a, tiles_x, tiles_y, err);
     return cudaGetLastError();
 }
@@ -747,11 +909,241 @@ cudaError_t conv_tc(const ConvArgs &a, int, unsigned *err, cudaStream_t st) {
     if (a.cin % 16 || a.cout % 16 || a.ldx % 16 || a.xoff % 16 || a.xoff + a.cin > a.ldx ||
         (a.y && (a.ldy % 16 || a.yoff % 16 || a.yoff + a.cout > a.ldy)) ||
         (a.yf && (a.ldyf % 16 || a.yfoff % 16 || a.yfoff + a.cout > a.ldyf)) ||
-        (a.ks != 1 && a.ks != 3) || a.B < 1 || a.H < 1 || a.W < 1)
+        (a.ks != 1 && a.ks != 3) || a.B < 1 || a.H < 1 || a.W < 1 || (a.up2 && !a.y))
         return cudaErrorInvalidValue;
     if (a.cin % 64 == 0) return conv_tc_n<64>(a, err, st);
     if (a.cin % 32 == 0) return conv_tc_n<32>(a, err, st);
     return conv_tc_n<16>(a, err, st);
+}
+
+// ---------------------------------------------------------------------------
+// Weight gradient on tcgen05:
+//   dw[co][m] += sum_p x[p + shift(tap)][ci] * dz[p][co],  m = tap * cin + ci.
+// GEMM rows = m (128 per block, as 128 / CA regions of CA channels of one tap),
+// columns = output channels (NT per block, NT / CB regions of CB channels),
+// K = pixels, one 8 x 16 patch per K step.  Both operands arrive as TMA boxes
+// {CA | CB channels, 16, 8, 1} of the NHWC tensors: pixel-major rows with the
+// channels contiguous, i.e. MN-major UMMA operands, one region per swizzle
+// atom column (leading byte offset = region size, stride byte offset = 8
+// pixel rows; a K = 16 MMA spans two 8-row groups).  The blocks of one
+// (row tile, column tile) split the patches between them and add their
+// accumulators to dw with FP32 atomics (coalesced along m).
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int wg_stages(int stage) {
+    return (200 * 1024) / stage < 2 ? 2 : ((200 * 1024) / stage > 6 ? 6 : (200 * 1024) / stage);
+}
+
+template <int CA, int NT>
+__global__ void __launch_bounds__(kTcThreads) k_wgrad_tc(const __grid_constant__ CUtensorMap tmx,
+                                                          const __grid_constant__ CUtensorMap tmz,
+                                                          WgArgs a, int tiles_x, int tiles_y,
+                                                          int n_mt, int n_nt, int per,
+                                                          unsigned *err) {
+    constexpr int CB = NT < 64 ? NT : 64;
+    constexpr int RA = kTcM / CA, RB = NT / CB;
+    constexpr int REGA = kTcM * CA * 2, REGB = kTcM * CB * 2;  // one box: 128 pixel rows
+    constexpr int A_BYTES = RA * REGA, B_BYTES = RB * REGB;
+    constexpr int STAGE = A_BYTES + B_BYTES;
+    constexpr int S = wg_stages(STAGE);
+    constexpr int TCOLS = NT < 32 ? 32 : NT;
+    constexpr uint32_t IDESC = umma_idesc_bf16(kTcM, NT) | (1u << 15) | (1u << 16);  // MN-major
+    constexpr unsigned SBOA = 8 * CA * 2, SBOB = 8 * CB * 2;
+    extern __shared__ unsigned char smraw[];
+    __shared__ __align__(8) uint64_t full[S], empty[S], done;
+    __shared__ uint32_t tmem_sh;
+    unsigned char *sm = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int u = blockIdx.x;
+    const int m0 = (u % n_mt) * kTcM, n0 = ((u / n_mt) % n_nt) * NT;
+    const int q0 = (u / (n_mt * n_nt)) * per;
+    const int M = a.ks * a.ks * a.cin;
+    const int nk = min(per, tiles_x * tiles_y * a.B - q0);  // >= 1 by the host's split
+    const int ra = min(RA, (M - m0) / CA);                   // regions holding rows < M
+    const int half = a.ks / 2;
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_sh)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&done, 1);
+        fence_mbar_init();
+    }
+    if (warp == 4 && lane == 0) {
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmx)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmz)) : "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_sh;
+
+    if (warp == 4) {
+        if (lane == 0) {  // TMA producer
+            bool ok = true;
+            for (int k = 0; k < nk; ++k) {
+                const int s = k % S;
+                const unsigned su = (unsigned)(k / S);
+                if (k >= S && !mbar_wait_tc(&empty[s], (su - 1) & 1)) ok = false;
+                int q = q0 + k;
+                const int x0 = (q % tiles_x) * kTileX;
+                q /= tiles_x;
+                const int y0 = (q % tiles_y) * kTileY, b = q / tiles_y;
+                unsigned char *sa = sm + s * STAGE;
+                mbar_arrive_expect_tx(&full[s], (unsigned)(ra * REGA + B_BYTES));
+                for (int j = 0; j < ra; ++j) {
+                    const int m = m0 + j * CA;
+                    const int tap = m / a.cin, c = m - tap * a.cin;
+                    tma_load_4d(sa + j * REGA, &tmx, c, x0 + tap % a.ks - half,
+                                y0 + tap / a.ks - half, b, &full[s]);
+                }
+                for (int j = 0; j < RB; ++j)
+                    tma_load_4d(sa + A_BYTES + j * REGB, &tmz, n0 + j * CB, x0, y0, b, &full[s]);
+            }
+            if (!ok && err) atomicOr(err, DEV_ERR_TIMEOUT);
+        }
+        __syncwarp();
+    } else if (warp == 5) {
+        if (lane == 0) {  // MMA issuer
+            bool ok = true;
+            for (int k = 0; k < nk; ++k) {
+                const int s = k % S;
+                if (!mbar_wait_tc(&full[s], (unsigned)(k / S) & 1)) ok = false;
+                tc_fence_after();
+                const unsigned sa = smem_u32(sm + s * STAGE);
+                const unsigned sb = sa + A_BYTES;
+#pragma unroll
+                for (int kk = 0; kk < kTcM / 16; ++kk) {  // 16 pixel rows per MMA
+                    const uint64_t da = umma_desc(sa + kk * 2 * SBOA, REGA, SBOA, sw_layout(CA));
+                    const uint64_t db = umma_desc(sb + kk * 2 * SBOB, REGB, SBOB, sw_layout(CB));
+                    const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
+                            tmem),
+                        "l"(da), "l"(db), "r"(IDESC), "r"(acc)
+                        : "memory");
+                }
+                asm volatile(
+                    "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 "
+                    "[%0];" ::"r"(smem_u32(&empty[s]))
+                    : "memory");
+            }
+            asm volatile(
+                "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                    smem_u32(&done))
+                : "memory");
+            if (!ok && err) atomicOr(err, DEV_ERR_TIMEOUT);
+        }
+        __syncwarp();
+    } else {  // epilogue: accumulator row r = GEMM row m0 + r
+        if (!mbar_wait_tc(&done, 0)) {
+            if (err && lane == 0) atomicOr(err, DEV_ERR_TIMEOUT);
+            mbar_wait_tc(&done, 0);  // once more, bounded
+        }
+        tc_fence_after();
+        const int m = m0 + warp * 32 + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < NT; c0 += 16) {
+            uint32_t v[16];
+            __syncwarp();
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+                "%12,%13,%14,%15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                  "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+                  "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < M) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                    atomicAdd(&a.dw[(size_t)(n0 + c0 + j) * M + m], __uint_as_float(v[j]));
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 5)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TCOLS)
+                     : "memory");
+}
+
+// Tensor map of a BF16 NHWC tensor's channel slice [0, C) (channel stride ld
+// elements) with boxes of {bc channels, 16, 8, 1}, swizzle span bc * 2 bytes.
+cudaError_t encode_nhwc(CUtensorMap *tm, const bf16 *base, int C, int ld, int W, int H, int B,
+                        int bc, CUtensorMapL2promotion l2) {
+    const auto enc = tmap_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    const cuuint64_t d[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    const cuuint64_t s[3] = {(cuuint64_t)ld * 2, (cuuint64_t)ld * 2 * W,
+                             (cuuint64_t)ld * 2 * W * H};
+    const cuuint32_t box[4] = {(cuuint32_t)bc, kTileX, kTileY, 1};
+    const cuuint32_t one[4] = {1, 1, 1, 1};
+    const CUtensorMapSwizzle swz = bc == 64   ? CU_TENSOR_MAP_SWIZZLE_128B
+                                   : bc == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                              : CU_TENSOR_MAP_SWIZZLE_32B;
+    if (enc(tm, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, (void *)base, d, s, box, one,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, swz, l2, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+        CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
+    return cudaSuccess;
+}
+
+template <int CA, int NT>
+cudaError_t launch_wgrad_tc(const WgArgs &a, unsigned *err, cudaStream_t st) {
+    constexpr int CB = NT < 64 ? NT : 64;
+    constexpr int STAGE = kTcM * kTcM * 2 + NT * kTcM * 2;
+    constexpr int SMEM = wg_stages(STAGE) * STAGE + 1024;
+    U_TRY(cudaFuncSetAttribute(k_wgrad_tc<CA, NT>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
+    CUtensorMap tmx, tmz;
+    U_TRY(encode_nhwc(&tmx, a.x + a.xoff, a.cin, a.ldx, a.W, a.H, a.B, CA,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B));
+    U_TRY(encode_nhwc(&tmz, a.dz, a.cout, a.cout, a.W, a.H, a.B, CB,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B));
+    int dev = 0, sms = 148;
+    U_TRY(cudaGetDevice(&dev));
+    U_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int tiles_x = (a.W + kTileX - 1) / kTileX, tiles_y = (a.H + kTileY - 1) / kTileY;
+    const long long n_patch = (long long)tiles_x * tiles_y * a.B;
+    const int n_mt = (a.ks * a.ks * a.cin + kTcM - 1) / kTcM, n_nt = a.cout / NT;
+    if (n_patch > 0x7fffffffLL) return cudaErrorInvalidValue;
+    // about two blocks per SM; every block gets at least one patch
+    const long long want = std::max(1LL, (2LL * sms + n_mt * n_nt - 1) / (n_mt * n_nt));
+    const int per = (int)((n_patch + want - 1) / want);
+    const int splits = (int)((n_patch + per - 1) / per);
+    k_wgrad_tc<CA, NT><<<n_mt * n_nt * splits, kTcThreads, SMEM, st>>>(
+        tmx, tmz, a, tiles_x, tiles_y, n_mt, n_nt, per, err);
+    return cudaGetLastError();
+}
+
+template <int CA>
+cudaError_t wgrad_tc_n(const WgArgs &a, unsigned *err, cudaStream_t st) {
+    if (a.cout == 16) return launch_wgrad_tc<CA, 16>(a, err, st);
+    if (a.cout == 32) return launch_wgrad_tc<CA, 32>(a, err, st);
+    if (a.cout == 64) return launch_wgrad_tc<CA, 64>(a, err, st);
+    return launch_wgrad_tc<CA, 128>(a, err, st);
+}
+
+// The tensor-memory weight gradient (accumulates into a.dw): cin and cout
+// multiples of 16, cout 16, 32, 64 or a multiple of 128.
+cudaError_t wgrad_tc(const WgArgs &a, unsigned *err, cudaStream_t st) {
+    if (a.cin % 16 || a.ldx % 16 || a.xoff % 16 || a.xoff + a.cin > a.ldx ||
+        !(a.cout == 16 || a.cout == 32 || a.cout == 64 || a.cout % 128 == 0) ||
+        (a.ks != 1 && a.ks != 3) || a.B < 1 || a.H < 1 || a.W < 1)
+        return cudaErrorInvalidValue;
+    if (a.cin % 64 == 0) return wgrad_tc_n<64>(a, err, st);
+    if (a.cin % 32 == 0) return wgrad_tc_n<32>(a, err, st);
+    return wgrad_tc_n<16>(a, err, st);
 }
 
 int gridn_u(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 32); }
@@ -759,12 +1151,6 @@ int gridn_u(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 32);
 constexpr int kLossBlocks = 296;
 
 }  // namespace
-
-#define U_TRY(x)                              \
-    do {                                      \
-        cudaError_t e_ = (x);                 \
-        if (e_ != cudaSuccess) return e_;     \
-    } while (0)
 
 UNet::~UNet() { release(); }
 
@@ -891,9 +1277,10 @@ cudaError_t UNet::sync_weights() {
     return cudaGetLastError();
 }
 
-cudaError_t UNet::conv_fwd(int li, const Act &in, int in_off, Act &out, int out_off) {
+cudaError_t UNet::conv_fwd(int li, const Act &in, int in_off, Act &out, int out_off, bool up2) {
     const ConvLayer &L = layers_[li];
     ConvArgs a{};
+    a.up2 = up2 ? 1 : 0;
     a.x = in.v;
     a.ldx = in.C;
     a.xoff = in_off;
@@ -939,7 +1326,7 @@ cudaError_t UNet::conv_bwd(int li, Act &in, int in_off, Act &out, int out_off) {
     const ConvLayer &L = layers_[li];
     const int P = B_ * in.H * in.W;
     const bool is_out = &out == &acts_[A_OUT];
-    k_dz<<<gridn_u((size_t)P * L.cout), 256, 0, st_>>>(
+    k_dz<<<gridn_u((size_t)P * L.cout / 8), 256, 0, st_>>>(
         dz_, is_out ? outg_ : out.g, out.C, is_out ? 0 : out_off, out.v, out.C,
         out_off, P, L.cout, L.relu ? 1 : 0);
     WgArgs w{};
@@ -954,10 +1341,17 @@ cudaError_t UNet::conv_bwd(int li, Act &in, int in_off, Act &out, int out_off) {
     w.cin = L.cin;
     w.cout = L.cout;
     w.ks = L.ks;
-    const int base = ((L.cout + 63) / 64) * ((L.cin + 63) / 64) * L.ks * L.ks;
-    w.splits = std::max(1, std::min((P + 31) / 32, 148 * 8 / base));
-    k_wgrad<<<dim3((L.cout + 63) / 64, (L.cin + 63) / 64, L.ks * L.ks * w.splits), kCT, 0, st_>>>(w);
-    k_bgrad<<<(P + 255) / 256, 256, 0, st_>>>(grad_ + L.b_off, dz_, P, L.cout);
+    if (use_tc_) {
+        U_TRY(wgrad_tc(w, err_, st_));
+    } else {
+        const int base = ((L.cout + 63) / 64) * ((L.cin + 63) / 64) * L.ks * L.ks;
+        w.splits = std::max(1, std::min((P + 31) / 32, 148 * 8 / base));
+        k_wgrad<<<dim3((L.cout + 63) / 64, (L.cin + 63) / 64, L.ks * L.ks * w.splits), kCT, 0,
+                   st_>>>(w);
+    }
+    const int lanes = 256 / (L.cout / 8);  // pixel lanes of a k_bgrad block
+    k_bgrad<<<std::min((P + lanes - 1) / lanes, 148 * 4), 256, 0, st_>>>(grad_ + L.b_off, dz_, P,
+                                                                         L.cout);
     launches_ += 3;
     if (li > 0 && in.g) {
         ConvArgs a{};
@@ -985,7 +1379,7 @@ cudaError_t UNet::conv_bwd(int li, Act &in, int in_off, Act &out, int out_off) {
 }
 
 cudaError_t UNet::pack_input(const float *x) {
-    k_pack<<<gridn_u((size_t)B_ * H_ * W_ * 16), 256, 0, st_>>>(acts_[A_X0].v, x, B_, H_ * W_);
+    k_pack<<<gridn_u((size_t)B_ * H_ * W_), 256, 0, st_>>>(acts_[A_X0].v, x, B_, H_ * W_);
     ++launches_;
     return cudaGetLastError();
 }
@@ -995,14 +1389,14 @@ cudaError_t UNet::run_forward() {
     auto pool = [&](int src, int lvl, int dst) {
         const Act &s = A[src];
         Act &d = A[dst];
-        k_pool_fwd<<<gridn_u((size_t)B_ * d.H * d.W * d.C), 256, 0, st_>>>(
+        k_pool_fwd<<<gridn_u((size_t)B_ * d.H * d.W * d.C / 8), 256, 0, st_>>>(
             d.v, pidx_ + pidx_off_[lvl], s.v, s.C, 0, B_, s.H, s.W, d.C);
         ++launches_;
     };
     auto up = [&](int src, int dst, int off) {
         const Act &s = A[src];
         Act &d = A[dst];
-        k_up_fwd<<<gridn_u((size_t)B_ * d.H * d.W * s.C), 256, 0, st_>>>(d.v, d.C, off, s.v, B_,
+        k_up_fwd<<<gridn_u((size_t)B_ * d.H * d.W * s.C / 8), 256, 0, st_>>>(d.v, d.C, off, s.v, B_,
                                                                        d.H, d.W, s.C);
         ++launches_;
     };
@@ -1017,16 +1411,22 @@ cudaError_t UNet::run_forward() {
     pool(A_D3, 2, A_P3);
     U_TRY(conv_fwd(6, A[A_P3], 0, A[A_M1], 0));
     U_TRY(conv_fwd(7, A[A_M1], 0, A[A_M2], 0));
-    U_TRY(conv_fwd(8, A[A_M2], 0, A[A_T3], 0));
-    up(A_T3, A_D3, 128);
+    // 1x1 conv then nearest x2 up-sampling into the upper channels of the skip
+    // buffer: fused into the tensor-memory kernel's epilogue (the backward pass
+    // needs only the up-sampled copy; these layers have no ReLU to mask).
+    auto conv_up = [&](int li, int src, int t, int dst, int off) -> cudaError_t {
+        if (use_tc_) return conv_fwd(li, A[src], 0, A[dst], off, true);
+        U_TRY(conv_fwd(li, A[src], 0, A[t], 0));
+        up(t, dst, off);
+        return cudaSuccess;
+    };
+    U_TRY(conv_up(8, A_M2, A_T3, A_D3, 128));
     U_TRY(conv_fwd(9, A[A_D3], 0, A[A_F3A], 0));
     U_TRY(conv_fwd(10, A[A_F3A], 0, A[A_F3B], 0));
-    U_TRY(conv_fwd(11, A[A_F3B], 0, A[A_T2], 0));
-    up(A_T2, A_D2, 64);
+    U_TRY(conv_up(11, A_F3B, A_T2, A_D2, 64));
     U_TRY(conv_fwd(12, A[A_D2], 0, A[A_F2A], 0));
     U_TRY(conv_fwd(13, A[A_F2A], 0, A[A_F2B], 0));
-    U_TRY(conv_fwd(14, A[A_F2B], 0, A[A_T1], 0));
-    up(A_T1, A_D1, 32);
+    U_TRY(conv_up(14, A_F2B, A_T1, A_D1, 32));
     U_TRY(conv_fwd(15, A[A_D1], 0, A[A_F1A], 0));
     U_TRY(conv_fwd(16, A[A_F1A], 0, A[A_F1B], 0));
     U_TRY(conv_fwd(17, A[A_F1B], 0, A[A_OUT], 0));
@@ -1068,14 +1468,14 @@ cudaError_t UNet::gradients(const float *x, const float *target, float *loss) {
     auto pool_bwd = [&](int dst, int lvl, int src) {  // gradient of pool(dst) -> dst.g
         Act &d = A[dst];
         const Act &s = A[src];
-        k_pool_bwd<<<gridn_u((size_t)B_ * s.H * s.W * s.C), 256, 0, st_>>>(
+        k_pool_bwd<<<gridn_u((size_t)B_ * s.H * s.W * s.C / 4), 256, 0, st_>>>(
             d.g, d.C, 0, s.g, pidx_ + pidx_off_[lvl], B_, d.H, d.W, s.C);
         ++launches_;
     };
     auto up_bwd = [&](int src, int dst, int off) {  // d(up(src) -> dst[off]) -> src.g
         Act &s = A[src];
         const Act &d = A[dst];
-        k_up_bwd<<<gridn_u((size_t)B_ * s.H * s.W * s.C), 256, 0, st_>>>(s.g, d.g, d.C, off, B_,
+        k_up_bwd<<<gridn_u((size_t)B_ * s.H * s.W * s.C / 4), 256, 0, st_>>>(s.g, d.g, d.C, off, B_,
                                                                         s.H, s.W, s.C);
         ++launches_;
     };

@@ -67,7 +67,9 @@ private:
         __nv_bfloat16 *v = nullptr;
         float *g = nullptr;
     };
-    cudaError_t conv_fwd(int li, const Act &in, int in_off, Act &out, int out_off);
+    // up2: out has twice in's size and receives the nearest x2 up-sampled output
+    cudaError_t conv_fwd(int li, const Act &in, int in_off, Act &out, int out_off,
+                         bool up2 = false);
     cudaError_t conv_bwd(int li, Act &in, int in_off, Act &out, int out_off);
     cudaError_t pack_input(const float *x);
     cudaError_t run_conv(const ConvArgs &a, int P);
