@@ -1117,8 +1117,13 @@ cudaError_t launch_wgrad_tc(const WgArgs &a, unsigned *err, cudaStream_t st) {
     const long long n_patch = (long long)tiles_x * tiles_y * a.B;
     const int n_mt = (a.ks * a.ks * a.cin + kTcM - 1) / kTcM, n_nt = a.cout / NT;
     if (n_patch > 0x7fffffffLL) return cudaErrorInvalidValue;
-    // about two blocks per SM; every block gets at least one patch
-    const long long want = std::max(1LL, (2LL * sms + n_mt * n_nt - 1) / (n_mt * n_nt));
+    // one full wave of resident blocks (no tail wave); every block gets at
+    // least one patch
+    int per_sm = 1;
+    U_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wgrad_tc<CA, NT>, kTcThreads,
+                                                        SMEM));
+    const long long wave = (long long)sms * std::max(per_sm, 1);
+    const long long want = std::max(1LL, wave / (n_mt * n_nt));
     const int per = (int)((n_patch + want - 1) / want);
     const int splits = (int)((n_patch + per - 1) / per);
     k_wgrad_tc<CA, NT><<<n_mt * n_nt * splits, kTcThreads, SMEM, st>>>(
