@@ -720,8 +720,8 @@ def run_batch(args, local):
                                f"{ms[:S]}); value = that time x {scale:.2f} (all 64 slices' "
                                f"samples / the timed slices' samples); 384x384, 32 coils, "
                                f"cg_num 20, no regularization",
-                   "parallelism": "one imp_bruteforce_batch call, solver cached per sample "
-                                  "count"},
+                   "parallelism": "one imp_bruteforce_batch call: all slices in lockstep, "
+                                  "one launch per CG step over every slice"},
         "gpu_launches": launches,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak, "traffic": None,

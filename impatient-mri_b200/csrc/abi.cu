@@ -247,7 +247,7 @@ imp_status imp_context_destroy(imp_context *ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->bf.reset();
-    ctx->bf_by_m.clear();
+    ctx->bb.reset();
     ctx->tp.reset();
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->dev_err) cudaFree(ctx->dev_err);
@@ -469,24 +469,15 @@ imp_status imp_bruteforce_batch(imp_context *ctx, const imp_bf_options *opt, flo
         d_sr = nullptr;  // one coil: unit sensitivity (kernels/structures.cpp:710-716)
         d_si = nullptr;
     }
-    long launches = 0;
-    for (int sl = 0; sl < num_slices; ++sl) {
-        const int Ms = k_off[sl + 1] - k_off[sl];
-        imp::BfConfig cfg;
-        if ((s = bf_config(opt, Ms, num_i, num_coil, &cfg)) != IMP_OK) return s;
-        // one solver per sample count: buffers, tuned shapes and graphs are
-        // reused by every slice of that size (and by later calls)
-        std::unique_ptr<imp::BfSolver> &slot = ctx->bf_by_m[Ms];
-        if (!slot) slot.reset(new imp::BfSolver());
-        const size_t o = (size_t)k_off[sl];
-        IMP_CUDA(slot->setup(cfg, d_kx + o, d_ky + o, d_kz ? d_kz + o : nullptr, d_t + o, d_ix,
-                             d_iy, d_iz, d_sr, d_si, ctx->dev_err, ctx->stream),
-                 "brute-force setup");
-        IMP_CUDA(slot->solve(d_fm ? d_fm + (size_t)sl * N : nullptr, d_kr + C * o, d_ki + C * o,
-                             d_xr + (size_t)sl * N, d_xi + (size_t)sl * N),
-                 "brute-force solve");
-        launches += slot->launches() + 4;
-    }
+    // all slices in lockstep: every CG step is one launch over all slices
+    imp::BfConfig cfg;
+    if ((s = bf_config(opt, k_off[1] - k_off[0], num_i, num_coil, &cfg)) != IMP_OK) return s;
+    if (!ctx->bb) ctx->bb.reset(new imp::BfBatch());
+    IMP_CUDA(ctx->bb->setup(cfg, num_slices, k_off, d_kx, d_ky, d_kz, d_t, d_ix, d_iy, d_iz, d_fm,
+                            d_sr, d_si, ctx->dev_err, ctx->stream),
+             "batched brute-force setup");
+    IMP_CUDA(ctx->bb->solve(d_kr, d_ki, d_xr, d_xi), "batched brute-force solve");
+    const long launches = ctx->bb->launches();
     if (x_host) {
         IMP_CUDA(cudaMemcpyAsync(idata_r, d_xr, S * N * sizeof(float), cudaMemcpyDeviceToHost,
                                  ctx->stream),

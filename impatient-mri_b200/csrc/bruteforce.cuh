@@ -75,4 +75,59 @@ private:
 
 constexpr int kDotBlocks = 296;  // 2 x 148 SMs, grid-stride
 
+// S independent slices sharing the image grid, the coil maps and the options,
+// each with its own trajectory (uneven sample counts), field map and data,
+// solved in lockstep (every slice runs the same cg_num / tv_num): each CG step
+// is ONE launch over all slices -- the batched NUDFT (blockIdx.z = slice x
+// coil group, per-slice offsets from a device table) or a vector kernel with
+// blockIdx.y = slice -- and every slice keeps its own FP64 scalars.  The
+// initialisation and the CG update are captured once as CUDA graphs.
+class BfBatch {
+public:
+    BfBatch() = default;
+    ~BfBatch();
+    BfBatch(const BfBatch &) = delete;
+    BfBatch &operator=(const BfBatch &) = delete;
+
+    // cfg.M is ignored.  Slice s owns samples k_off[s] .. k_off[s+1]-1 (host
+    // array) of the device SoA trajectory arrays; fm: [S][N] (or null).
+    cudaError_t setup(const BfConfig &cfg, int S, const int *k_off, const float *kx,
+                      const float *ky, const float *kz, const float *t, const float *ix,
+                      const float *iy, const float *iz, const float *fm, const float *sensi_r,
+                      const float *sensi_i, unsigned *dev_err, cudaStream_t st);
+    // kdata: slice s's [C][M_s] block at C * k_off[s]; x: [S][N] SoA in/out.
+    cudaError_t solve(const float *kd_r, const float *kd_i, float *x_r, float *x_i);
+
+    long launches() const { return launches_; }
+    int slices() const { return S_; }
+    void release();
+
+private:
+    cudaError_t run_init();
+    cudaError_t run_iteration();
+
+    BfConfig cfg_;
+    NuPlan plan_;          // C, CG, G, Npad, use_z and the shared sensitivities
+    NuLaunch fwd_, adj_;   // one launch shape for all slices
+    int S_ = 0, kb_ = 1;   // slices; vector-kernel blocks per slice
+    int max_mpad_ = 0;
+    long long mpad_total_ = 0;  // sum of the slices' padded sample counts
+    std::vector<int> k_off_, m_, mpad_;
+    std::vector<long long> koff_pad_;
+    cudaStream_t st_ = nullptr;
+    unsigned *err_ = nullptr;
+    double4 *kgeo_ = nullptr, *vgeo_ = nullptr;
+    float2 *sens_ = nullptr;
+    NuSlice *tab_fwd_ = nullptr, *tab_adj_ = nullptr;
+    void *tab_vec_ = nullptr;  // per-slice (padded offset, M, Mpad) of the vector kernels
+    float2 *y_ = nullptr, *af_ = nullptr, *q_ = nullptr, *rpk_ = nullptr, *xs_ = nullptr;
+    float2 *x_ = nullptr, *g_ = nullptr, *d_ = nullptr;
+    float *w_ = nullptr;
+    float2 *pf_ = nullptr, *pa_ = nullptr;
+    double *dots_ = nullptr;  // [S][5][kb_]
+    cudaGraphExec_t g_iter_ = nullptr, g_init_ = nullptr;
+    long launches_ = 0;
+    int per_iter_launches_ = 0, per_init_launches_ = 0;
+};
+
 }  // namespace imp

@@ -10,6 +10,7 @@
 
 namespace imp {
 class BfSolver;
+class BfBatch;
 class ToepSolver;
 }  // namespace imp
 
@@ -24,7 +25,7 @@ struct imp_context {
     double prof_ms[2] = {0.0, 0.0};
     long prof_count[2] = {0, 0};
     std::unique_ptr<imp::BfSolver> bf;    // brute-force solver reused across calls
-    std::map<int, std::unique_ptr<imp::BfSolver>> bf_by_m;  // batched slices, per sample count
+    std::unique_ptr<imp::BfBatch> bb;     // batched multi-slice solver
     std::unique_ptr<imp::ToepSolver> tp;  // Toeplitz solver reused across calls
     ~imp_context();
 };

@@ -30,18 +30,33 @@ constexpr double kMagic = 1572864.0 + 0.5 + 5.9604644775390625e-08;
 constexpr float kTwoPiF = 6.28318530717958647692f;
 constexpr float kThreePiF = 9.42477796076937971538f;
 
-template <int CG, int PT, bool USEZ, bool ADJ, int OCC>
+// BATCH: blockIdx.z = slice * G + coil group; the slice's offsets and padded
+// sizes come from sl[slice] (blocks past the slice's "ours" range exit).
+template <int CG, int PT, bool USEZ, bool ADJ, int OCC, bool BATCH>
 __global__ void __launch_bounds__(kNT, OCC)
     k_nudft(const double4 *__restrict__ ours, const double4 *__restrict__ theirs,
             const float2 *__restrict__ tdata, const float2 *__restrict__ sens,
             float2 *__restrict__ out, int n_ours_pad, int n_theirs_pad, int per_split,
-            unsigned *err) {
+            unsigned *err, const NuSlice *__restrict__ sl, int n_groups) {
     __shared__ __align__(128) double4 s_geo[2][kTile];
     __shared__ __align__(128) float2 s_dat[2][kTile * CG];
     __shared__ __align__(8) uint64_t s_bar[2];
 
     const int tid = threadIdx.x;
-    const int g = blockIdx.z;
+    int g = blockIdx.z;
+    if constexpr (BATCH) {
+        const int s = blockIdx.z / n_groups;
+        g = blockIdx.z - s * n_groups;
+        const NuSlice d = sl[s];
+        if (blockIdx.x * (kNT * PT) >= d.n_ours) return;  // whole block: before any barrier
+        ours += d.ours;
+        theirs += d.theirs;
+        tdata += d.tdata;
+        out += d.out;
+        n_ours_pad = d.n_ours;
+        n_theirs_pad = d.n_theirs;
+        per_split = d.per_split;
+    }
     const int split = blockIdx.y;
     const int e0 = blockIdx.x * (kNT * PT) + tid;
 
@@ -133,7 +148,7 @@ __global__ void __launch_bounds__(kNT, OCC)
         __syncthreads();
     }
 
-    const int G = gridDim.z;
+    const int G = BATCH ? n_groups : (int)gridDim.z;
     if (!ADJ) {
         float2 *o = out + ((size_t)(split * G + g) * n_ours_pad) * CG;
 #pragma unroll
@@ -309,12 +324,53 @@ cudaError_t launch_cg_pt(const NuPlan &p, int split, const double4 *ours, const 
     const int per_split = n_theirs / split;
     dim3 grid(n_ours / (kNT * PT), split, p.G);
     if (p.use_z)
-        k_nudft<CG, PT, true, ADJ, OCC><<<grid, kNT, 0, st>>>(ours, theirs, tdata, p.sens, out,
-                                                              n_ours, n_theirs, per_split, err);
+        k_nudft<CG, PT, true, ADJ, OCC, false><<<grid, kNT, 0, st>>>(
+            ours, theirs, tdata, p.sens, out, n_ours, n_theirs, per_split, err, nullptr, p.G);
     else
-        k_nudft<CG, PT, false, ADJ, OCC><<<grid, kNT, 0, st>>>(ours, theirs, tdata, p.sens, out,
-                                                               n_ours, n_theirs, per_split, err);
+        k_nudft<CG, PT, false, ADJ, OCC, false><<<grid, kNT, 0, st>>>(
+            ours, theirs, tdata, p.sens, out, n_ours, n_theirs, per_split, err, nullptr, p.G);
     return cudaGetLastError();
+}
+
+// Batched: S slices sharing N, C and the sensitivities; `max_ours` is the
+// largest padded "ours" count of a slice.
+template <int CG, int PT, bool ADJ, int OCC>
+cudaError_t launch_cg_pt_batch(const NuPlan &p, int split, int S, int max_ours,
+                               const NuSlice *sl, const double4 *ours, const double4 *theirs,
+                               const float2 *tdata, float2 *out, unsigned *err,
+                               cudaStream_t st) {
+    if ((long long)S * p.G > 65535 || max_ours % (kNT * PT)) return cudaErrorInvalidConfiguration;
+    dim3 grid(max_ours / (kNT * PT), split, S * p.G);
+    if (p.use_z)
+        k_nudft<CG, PT, true, ADJ, OCC, true><<<grid, kNT, 0, st>>>(
+            ours, theirs, tdata, p.sens, out, 0, 0, 0, err, sl, p.G);
+    else
+        k_nudft<CG, PT, false, ADJ, OCC, true><<<grid, kNT, 0, st>>>(
+            ours, theirs, tdata, p.sens, out, 0, 0, 0, err, sl, p.G);
+    return cudaGetLastError();
+}
+
+template <bool ADJ>
+cudaError_t launch_nudft_batch(const NuPlan &p, const NuLaunch &l, int S, int max_ours,
+                               const NuSlice *sl, const double4 *ours, const double4 *theirs,
+                               const float2 *tdata, float2 *out, unsigned *err,
+                               cudaStream_t st) {
+#define IMP_CASE(CGV, PTV)                                                                     \
+    if (p.CG == CGV && l.pt == PTV) {                                                          \
+        if (l.occ == 6)                                                                        \
+            return launch_cg_pt_batch<CGV, PTV, ADJ, 6>(p, l.split, S, max_ours, sl, ours,     \
+                                                        theirs, tdata, out, err, st);          \
+        return launch_cg_pt_batch<CGV, PTV, ADJ, 4>(p, l.split, S, max_ours, sl, ours, theirs, \
+                                                    tdata, out, err, st);                      \
+    }
+    IMP_CASE(1, 4)
+    IMP_CASE(1, 8)
+    IMP_CASE(2, 4)
+    IMP_CASE(4, 2)
+    IMP_CASE(4, 4)
+    IMP_CASE(8, 2)
+#undef IMP_CASE
+    return cudaErrorInvalidConfiguration;
 }
 
 template <bool ADJ>
@@ -484,6 +540,17 @@ cudaError_t nu_forward_partials(const NuPlan &p, const NuLaunch &l, const float2
 cudaError_t nu_adjoint_partials(const NuPlan &p, const NuLaunch &l, const float2 *data,
                                 float2 *part, unsigned *dev_err, cudaStream_t st) {
     return launch_nudft<true>(p, l, data, part, dev_err, st);
+}
+
+cudaError_t nu_partials_batch(const NuPlan &p, const NuLaunch &l, bool adj, int S, int max_ours,
+                              const NuSlice *d_slices, const double4 *ours,
+                              const double4 *theirs, const float2 *tdata, float2 *part,
+                              unsigned *dev_err, cudaStream_t st) {
+    if (S < 1 || !d_slices) return cudaErrorInvalidValue;
+    return adj ? launch_nudft_batch<true>(p, l, S, max_ours, d_slices, ours, theirs, tdata, part,
+                                          dev_err, st)
+               : launch_nudft_batch<false>(p, l, S, max_ours, d_slices, ours, theirs, tdata,
+                                           part, dev_err, st);
 }
 
 cudaError_t nu_pack_kdata(const NuPlan &p, const float *dr, const float *di, float2 *packed,

@@ -85,6 +85,24 @@ cudaError_t nu_forward_partials(const NuPlan &p, const NuLaunch &l, const float2
 cudaError_t nu_adjoint_partials(const NuPlan &p, const NuLaunch &l, const float2 *data,
                                 float2 *part, unsigned *dev_err, cudaStream_t st);
 
+// One slice of a batched launch: element offsets into the concatenated
+// "ours" / "theirs" geometry (double4), the "theirs" data and the partial
+// sums (float2), and the slice's padded sizes.
+struct NuSlice {
+    long long ours, theirs, tdata, out;
+    int n_ours, n_theirs, per_split;
+};
+
+// Partials of S slices in one launch (grid: max_ours / (kNT * pt) x split x
+// S * G); `p` supplies C, CG, G, use_z and the shared sensitivities, `l` the
+// launch shape (its split must cut every slice's "theirs" range into whole
+// tiles).  Per-slice layouts are those of nu_forward_partials /
+// nu_adjoint_partials at the slice's offsets.
+cudaError_t nu_partials_batch(const NuPlan &p, const NuLaunch &l, bool adj, int S, int max_ours,
+                              const NuSlice *d_slices, const double4 *ours,
+                              const double4 *theirs, const float2 *tdata, float2 *part,
+                              unsigned *dev_err, cudaStream_t st);
+
 // k-space SoA [C][M] <-> packed [G][Mpad][CG]
 cudaError_t nu_pack_kdata(const NuPlan &p, const float *dr, const float *di, float2 *packed,
                           cudaStream_t st);

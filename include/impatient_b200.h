@@ -166,8 +166,9 @@ imp_status imp_bruteforce_recon(imp_context *ctx, const imp_bf_options *opt, flo
  * samples k_off[s] .. k_off[s+1]-1 of kx, ky, kz, t (k_off: host array of
  * num_slices+1 offsets, k_off[0] = 0); its data are
  * kdata[num_coil*k_off[s] + c*(k_off[s+1]-k_off[s]) + k]; fm and idata are
- * [slice][num_i].  The context keeps one solver per distinct sample count, so
- * buffers, tuned shapes and CUDA graphs are reused by every slice of that size. */
+ * [slice][num_i].  All slices are solved in lockstep: every CG step is one
+ * kernel launch over all slices (uneven sample counts included), each slice
+ * with its own FP64 CG scalars; the CG update is a CUDA graph. */
 imp_status imp_bruteforce_batch(imp_context *ctx, const imp_bf_options *opt, float *idata_r,
                                 float *idata_i, const float *kdata_r, const float *kdata_i,
                                 const float *kx, const float *ky, const float *kz,
