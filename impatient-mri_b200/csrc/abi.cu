@@ -37,6 +37,9 @@ imp_status from_cuda(cudaError_t e, const char *what) {
 imp_status begin(imp_context *ctx) {
     if (!ctx) return fail(IMP_ERR_INVALID_ARG, "null context");
     IMP_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    // a call that failed part-way may have left work queued that reads the
+    // staging arena this call is about to refill
+    IMP_CUDA(cudaStreamSynchronize(ctx->stream), "stream synchronize");
     IMP_CUDA(cudaMemsetAsync(ctx->dev_err, 0, sizeof(unsigned), ctx->stream), "clear error word");
     ctx->launches = 0;
     return IMP_OK;
@@ -183,6 +186,49 @@ imp_status to_device(imp_context *ctx, const float *p, size_t n, DevKeep &keep,
     return IMP_OK;
 }
 
+void stage_reset(imp_context *ctx) {
+    ctx->stage_chunk = 0;
+    ctx->stage_off = 0;
+}
+
+static imp_status stage_alloc(imp_context *ctx, size_t bytes, void **out) {
+    bytes = (bytes + 255) & ~(size_t)255;
+    while (ctx->stage_chunk < ctx->stage.size()) {
+        const auto &c = ctx->stage[ctx->stage_chunk];
+        if (ctx->stage_off + bytes <= c.second) {
+            *out = (char *)c.first + ctx->stage_off;
+            ctx->stage_off += bytes;
+            return IMP_OK;
+        }
+        ++ctx->stage_chunk;
+        ctx->stage_off = 0;
+    }
+    const size_t cap = std::max(bytes, (size_t)64 << 20);
+    void *d = nullptr;
+    IMP_CUDA(cudaMalloc(&d, cap), "staging arena");
+    ctx->stage.emplace_back(d, cap);
+    ctx->stage_chunk = ctx->stage.size() - 1;
+    ctx->stage_off = bytes;
+    *out = d;
+    return IMP_OK;
+}
+
+imp_status to_device_staged(imp_context *ctx, const float *p, size_t n, const float **out,
+                            bool *was_host) {
+    *out = p;
+    if (was_host) *was_host = false;
+    if (!p || n == 0) return IMP_OK;
+    if (is_device_ptr(p)) return IMP_OK;
+    void *d = nullptr;
+    imp_status s = stage_alloc(ctx, n * sizeof(float), &d);
+    if (s != IMP_OK) return s;
+    IMP_CUDA(cudaMemcpyAsync(d, p, n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream),
+             "input H2D");
+    *out = (const float *)d;
+    if (was_host) *was_host = true;
+    return IMP_OK;
+}
+
 imp_status out_device(imp_context *ctx, float *p, size_t n, DevKeep &keep, float **out,
                       bool *was_host) {
     (void)ctx;
@@ -200,7 +246,9 @@ imp_status out_device(imp_context *ctx, float *p, size_t n, DevKeep &keep, float
 
 }  // namespace imp
 
+using imp::stage_reset;
 using imp::to_device;
+using imp::to_device_staged;
 
 extern "C" {
 
@@ -249,6 +297,8 @@ imp_status imp_context_destroy(imp_context *ctx) {
     ctx->bf.reset();
     ctx->bb.reset();
     ctx->tp.reset();
+    for (auto &c : ctx->stage) cudaFree(c.first);
+    ctx->stage.clear();
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->dev_err) cudaFree(ctx->dev_err);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -365,25 +415,25 @@ imp_status imp_bruteforce_recon(imp_context *ctx, const imp_bf_options *opt, flo
     imp::BfConfig cfg;
     if ((s = bf_config(opt, num_k, num_i, num_coil, &cfg)) != IMP_OK) return s;
     if ((s = begin(ctx)) != IMP_OK) return s;
-    std::vector<std::unique_ptr<void, void (*)(void *)>> keep;
     const size_t M = num_k, N = num_i, C = num_coil, S = num_slices;
     const float *d_kx, *d_ky, *d_kz = nullptr, *d_ix, *d_iy, *d_iz = nullptr, *d_t, *d_fm = nullptr;
     const float *d_sr = nullptr, *d_si = nullptr, *d_kr, *d_ki, *d_xr0, *d_xi0;
     bool x_host = false, dummy;
-    if ((s = to_device(ctx, kx, M, keep, &d_kx, &dummy)) ||
-        (s = to_device(ctx, ky, M, keep, &d_ky, &dummy)) ||
-        (s = to_device(ctx, kz, M, keep, &d_kz, &dummy)) ||
-        (s = to_device(ctx, t, M, keep, &d_t, &dummy)) ||
-        (s = to_device(ctx, ix, N, keep, &d_ix, &dummy)) ||
-        (s = to_device(ctx, iy, N, keep, &d_iy, &dummy)) ||
-        (s = to_device(ctx, iz, N, keep, &d_iz, &dummy)) ||
-        (s = to_device(ctx, fm, S * N, keep, &d_fm, &dummy)) ||
-        (s = to_device(ctx, sensi_r, C * N, keep, &d_sr, &dummy)) ||
-        (s = to_device(ctx, sensi_i, C * N, keep, &d_si, &dummy)) ||
-        (s = to_device(ctx, kdata_r, S * C * M, keep, &d_kr, &dummy)) ||
-        (s = to_device(ctx, kdata_i, S * C * M, keep, &d_ki, &dummy)) ||
-        (s = to_device(ctx, idata_r, S * N, keep, &d_xr0, &x_host)) ||
-        (s = to_device(ctx, idata_i, S * N, keep, &d_xi0, &dummy)))
+    stage_reset(ctx);
+    if ((s = to_device_staged(ctx, kx, M, &d_kx, &dummy)) ||
+        (s = to_device_staged(ctx, ky, M, &d_ky, &dummy)) ||
+        (s = to_device_staged(ctx, kz, M, &d_kz, &dummy)) ||
+        (s = to_device_staged(ctx, t, M, &d_t, &dummy)) ||
+        (s = to_device_staged(ctx, ix, N, &d_ix, &dummy)) ||
+        (s = to_device_staged(ctx, iy, N, &d_iy, &dummy)) ||
+        (s = to_device_staged(ctx, iz, N, &d_iz, &dummy)) ||
+        (s = to_device_staged(ctx, fm, S * N, &d_fm, &dummy)) ||
+        (s = to_device_staged(ctx, sensi_r, C * N, &d_sr, &dummy)) ||
+        (s = to_device_staged(ctx, sensi_i, C * N, &d_si, &dummy)) ||
+        (s = to_device_staged(ctx, kdata_r, S * C * M, &d_kr, &dummy)) ||
+        (s = to_device_staged(ctx, kdata_i, S * C * M, &d_ki, &dummy)) ||
+        (s = to_device_staged(ctx, idata_r, S * N, &d_xr0, &x_host)) ||
+        (s = to_device_staged(ctx, idata_i, S * N, &d_xi0, &dummy)))
         return s;
     float *d_xr = const_cast<float *>(d_xr0), *d_xi = const_cast<float *>(d_xi0);
     if (num_coil == 1) {
@@ -444,25 +494,25 @@ imp_status imp_bruteforce_batch(imp_context *ctx, const imp_bf_options *opt, flo
     if (opt->cg_num <= 0) return fail(IMP_ERR_INVALID_ARG, "cg_num must be > 0");
     if (opt->enable_tv && opt->tv_num <= 0) return fail(IMP_ERR_INVALID_ARG, "tv_num must be > 0");
     if ((s = begin(ctx)) != IMP_OK) return s;
-    std::vector<std::unique_ptr<void, void (*)(void *)>> keep;
     const size_t N = num_i, C = num_coil, S = num_slices;
     const float *d_kx, *d_ky, *d_kz = nullptr, *d_ix, *d_iy, *d_iz = nullptr, *d_t, *d_fm = nullptr;
     const float *d_sr = nullptr, *d_si = nullptr, *d_kr, *d_ki, *d_xr0, *d_xi0;
     bool x_host = false, dummy;
-    if ((s = to_device(ctx, kx, Mt, keep, &d_kx, &dummy)) ||
-        (s = to_device(ctx, ky, Mt, keep, &d_ky, &dummy)) ||
-        (s = to_device(ctx, kz, Mt, keep, &d_kz, &dummy)) ||
-        (s = to_device(ctx, t, Mt, keep, &d_t, &dummy)) ||
-        (s = to_device(ctx, ix, N, keep, &d_ix, &dummy)) ||
-        (s = to_device(ctx, iy, N, keep, &d_iy, &dummy)) ||
-        (s = to_device(ctx, iz, N, keep, &d_iz, &dummy)) ||
-        (s = to_device(ctx, fm, S * N, keep, &d_fm, &dummy)) ||
-        (s = to_device(ctx, sensi_r, C * N, keep, &d_sr, &dummy)) ||
-        (s = to_device(ctx, sensi_i, C * N, keep, &d_si, &dummy)) ||
-        (s = to_device(ctx, kdata_r, C * Mt, keep, &d_kr, &dummy)) ||
-        (s = to_device(ctx, kdata_i, C * Mt, keep, &d_ki, &dummy)) ||
-        (s = to_device(ctx, idata_r, S * N, keep, &d_xr0, &x_host)) ||
-        (s = to_device(ctx, idata_i, S * N, keep, &d_xi0, &dummy)))
+    stage_reset(ctx);
+    if ((s = to_device_staged(ctx, kx, Mt, &d_kx, &dummy)) ||
+        (s = to_device_staged(ctx, ky, Mt, &d_ky, &dummy)) ||
+        (s = to_device_staged(ctx, kz, Mt, &d_kz, &dummy)) ||
+        (s = to_device_staged(ctx, t, Mt, &d_t, &dummy)) ||
+        (s = to_device_staged(ctx, ix, N, &d_ix, &dummy)) ||
+        (s = to_device_staged(ctx, iy, N, &d_iy, &dummy)) ||
+        (s = to_device_staged(ctx, iz, N, &d_iz, &dummy)) ||
+        (s = to_device_staged(ctx, fm, S * N, &d_fm, &dummy)) ||
+        (s = to_device_staged(ctx, sensi_r, C * N, &d_sr, &dummy)) ||
+        (s = to_device_staged(ctx, sensi_i, C * N, &d_si, &dummy)) ||
+        (s = to_device_staged(ctx, kdata_r, C * Mt, &d_kr, &dummy)) ||
+        (s = to_device_staged(ctx, kdata_i, C * Mt, &d_ki, &dummy)) ||
+        (s = to_device_staged(ctx, idata_r, S * N, &d_xr0, &x_host)) ||
+        (s = to_device_staged(ctx, idata_i, S * N, &d_xi0, &dummy)))
         return s;
     float *d_xr = const_cast<float *>(d_xr0), *d_xi = const_cast<float *>(d_xi0);
     if (num_coil == 1) {

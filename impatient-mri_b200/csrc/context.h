@@ -27,6 +27,11 @@ struct imp_context {
     std::unique_ptr<imp::BfSolver> bf;    // brute-force solver reused across calls
     std::unique_ptr<imp::BfBatch> bb;     // batched multi-slice solver
     std::unique_ptr<imp::ToepSolver> tp;  // Toeplitz solver reused across calls
+    // Grow-only staging arena for the host inputs / outputs of the brute-force
+    // entry points (which call no other entry point): chunks are kept across
+    // calls, so repeated calls of one size allocate nothing.
+    std::vector<std::pair<void *, size_t>> stage;
+    size_t stage_chunk = 0, stage_off = 0;
     ~imp_context();
 };
 
@@ -48,6 +53,11 @@ imp_status to_device(imp_context *ctx, const float *p, size_t n, DevKeep &keep,
 // A writable device buffer for an output that may live in host memory.
 imp_status out_device(imp_context *ctx, float *p, size_t n, DevKeep &keep, float **out,
                       bool *was_host);
+// to_device through the context's staging arena (no allocation once the arena
+// has grown to the call's size); stage_reset starts a call's arena use.
+void stage_reset(imp_context *ctx);
+imp_status to_device_staged(imp_context *ctx, const float *p, size_t n, const float **out,
+                            bool *was_host);
 
 }  // namespace imp
 
