@@ -229,6 +229,19 @@ imp_status to_device_staged(imp_context *ctx, const float *p, size_t n, const fl
     return IMP_OK;
 }
 
+imp_status out_device_staged(imp_context *ctx, float *p, size_t n, float **out, bool *was_host) {
+    *out = p;
+    *was_host = false;
+    if (!p || n == 0) return IMP_OK;
+    if (is_device_ptr(p)) return IMP_OK;
+    void *d = nullptr;
+    imp_status s = stage_alloc(ctx, n * sizeof(float), &d);
+    if (s != IMP_OK) return s;
+    *out = (float *)d;
+    *was_host = true;
+    return IMP_OK;
+}
+
 imp_status out_device(imp_context *ctx, float *p, size_t n, DevKeep &keep, float **out,
                       bool *was_host) {
     (void)ctx;
@@ -297,6 +310,7 @@ imp_status imp_context_destroy(imp_context *ctx) {
     ctx->bf.reset();
     ctx->bb.reset();
     ctx->tp.reset();
+    ctx->tp_q.reset();
     for (auto &c : ctx->stage) cudaFree(c.first);
     ctx->stage.clear();
     if (ctx->scratch) cudaFree(ctx->scratch);

@@ -27,6 +27,7 @@ struct imp_context {
     std::unique_ptr<imp::BfSolver> bf;    // brute-force solver reused across calls
     std::unique_ptr<imp::BfBatch> bb;     // batched multi-slice solver
     std::unique_ptr<imp::ToepSolver> tp;  // Toeplitz solver reused across calls
+    std::unique_ptr<imp::ToepSolver> tp_q;  // Toeplitz Q gridding (one coil)
     // Grow-only staging arena for the host inputs / outputs of the brute-force
     // entry points (which call no other entry point): chunks are kept across
     // calls, so repeated calls of one size allocate nothing.
@@ -58,6 +59,7 @@ imp_status out_device(imp_context *ctx, float *p, size_t n, DevKeep &keep, float
 void stage_reset(imp_context *ctx);
 imp_status to_device_staged(imp_context *ctx, const float *p, size_t n, const float **out,
                             bool *was_host);
+imp_status out_device_staged(imp_context *ctx, float *p, size_t n, float **out, bool *was_host);
 
 }  // namespace imp
 

@@ -970,6 +970,14 @@ imp::ToepSolver &solver_of(imp_context *ctx) {
     return *ctx->tp;
 }
 
+// Q is coil-free: it gets its own solver, so that alternating Q and
+// F^H d / CG calls (one coil versus num_coil) keep both set up instead of
+// rebuilding buffers and FFT plans on every call.
+imp::ToepSolver &solver_q_of(imp_context *ctx) {
+    if (!ctx->tp_q) ctx->tp_q.reset(new imp::ToepSolver());
+    return *ctx->tp_q;
+}
+
 imp_status copy_out(imp_context *ctx, float *dst, const float *src, size_t n) {
     IMP_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream),
              "output D2H");
@@ -999,22 +1007,23 @@ imp_status imp_toeplitz_q(imp_context *ctx, const imp_toeplitz_options *opt, flo
     if (!q_r || !q_i || !kx || !ky || !t || (nz > 1 && !kz))
         return fail(IMP_ERR_INVALID_ARG, "null array argument");
     if ((s = imp::begin(ctx)) != IMP_OK) return s;
+    imp::stage_reset(ctx);
     DevKeep keep;
     const float *dkx, *dky, *dkz = nullptr, *dt;
-    if ((s = imp::to_device(ctx, kx, num_k, keep, &dkx, nullptr)) ||
-        (s = imp::to_device(ctx, ky, num_k, keep, &dky, nullptr)) ||
-        (s = imp::to_device(ctx, kz, nz > 1 ? num_k : 0, keep, &dkz, nullptr)) ||
-        (s = imp::to_device(ctx, t, num_k, keep, &dt, nullptr)))
+    if ((s = imp::to_device_staged(ctx, kx, num_k, &dkx, nullptr)) ||
+        (s = imp::to_device_staged(ctx, ky, num_k, &dky, nullptr)) ||
+        (s = imp::to_device_staged(ctx, kz, nz > 1 ? num_k : 0, &dkz, nullptr)) ||
+        (s = imp::to_device_staged(ctx, t, num_k, &dt, nullptr)))
         return s;
-    imp::ToepSolver &ts = solver_of(ctx);
+    imp::ToepSolver &ts = solver_q_of(ctx);
     IMP_CUDA(ts.setup(toep_cfg(opt, nx, ny, nz, 1, num_k), dt, nullptr, nullptr, nullptr,
                       ctx->dev_err, ctx->stream),
              "toeplitz setup");
     const size_t nq = (size_t)ts.segments() * ts.q_elems();
     float *dqr, *dqi;
     bool hr, hi;
-    if ((s = imp::out_device(ctx, q_r, nq, keep, &dqr, &hr)) ||
-        (s = imp::out_device(ctx, q_i, nq, keep, &dqi, &hi)))
+    if ((s = imp::out_device_staged(ctx, q_r, nq, &dqr, &hr)) ||
+        (s = imp::out_device_staged(ctx, q_i, nq, &dqi, &hi)))
         return s;
     IMP_CUDA(ts.compute_q(dkx, dky, dkz, dqr, dqi), "Q gridding");
     if (hr && (s = copy_out(ctx, q_r, dqr, nq))) return s;
@@ -1036,19 +1045,20 @@ imp_status imp_toeplitz_fhd(imp_context *ctx, const imp_toeplitz_options *opt, f
     if (num_coil <= 0 || (num_coil > 1 && (!sensi_r || !sensi_i)))
         return fail(IMP_ERR_INVALID_ARG, "num_coil > 0 and sensi for num_coil > 1");
     if ((s = imp::begin(ctx)) != IMP_OK) return s;
+    imp::stage_reset(ctx);
     const size_t N = (size_t)nx * ny * nz, M = num_k, C = num_coil;
     DevKeep keep;
     const float *dkx, *dky, *dkz = nullptr, *dt, *dfm = nullptr, *dsr = nullptr, *dsi = nullptr,
                       *dkr, *dki;
-    if ((s = imp::to_device(ctx, kx, M, keep, &dkx, nullptr)) ||
-        (s = imp::to_device(ctx, ky, M, keep, &dky, nullptr)) ||
-        (s = imp::to_device(ctx, kz, nz > 1 ? M : 0, keep, &dkz, nullptr)) ||
-        (s = imp::to_device(ctx, t, M, keep, &dt, nullptr)) ||
-        (s = imp::to_device(ctx, fm, N, keep, &dfm, nullptr)) ||
-        (s = imp::to_device(ctx, num_coil > 1 ? sensi_r : nullptr, C * N, keep, &dsr, nullptr)) ||
-        (s = imp::to_device(ctx, num_coil > 1 ? sensi_i : nullptr, C * N, keep, &dsi, nullptr)) ||
-        (s = imp::to_device(ctx, kdata_r, C * M, keep, &dkr, nullptr)) ||
-        (s = imp::to_device(ctx, kdata_i, C * M, keep, &dki, nullptr)))
+    if ((s = imp::to_device_staged(ctx, kx, M, &dkx, nullptr)) ||
+        (s = imp::to_device_staged(ctx, ky, M, &dky, nullptr)) ||
+        (s = imp::to_device_staged(ctx, kz, nz > 1 ? M : 0, &dkz, nullptr)) ||
+        (s = imp::to_device_staged(ctx, t, M, &dt, nullptr)) ||
+        (s = imp::to_device_staged(ctx, fm, N, &dfm, nullptr)) ||
+        (s = imp::to_device_staged(ctx, num_coil > 1 ? sensi_r : nullptr, C * N, &dsr, nullptr)) ||
+        (s = imp::to_device_staged(ctx, num_coil > 1 ? sensi_i : nullptr, C * N, &dsi, nullptr)) ||
+        (s = imp::to_device_staged(ctx, kdata_r, C * M, &dkr, nullptr)) ||
+        (s = imp::to_device_staged(ctx, kdata_i, C * M, &dki, nullptr)))
         return s;
     imp::ToepSolver &ts = solver_of(ctx);
     IMP_CUDA(ts.setup(toep_cfg(opt, nx, ny, nz, num_coil, num_k), dt, dfm, dsr, dsi,
@@ -1056,8 +1066,8 @@ imp_status imp_toeplitz_fhd(imp_context *ctx, const imp_toeplitz_options *opt, f
              "toeplitz setup");
     float *dfr, *dfi;
     bool hr, hi;
-    if ((s = imp::out_device(ctx, fhd_r, N, keep, &dfr, &hr)) ||
-        (s = imp::out_device(ctx, fhd_i, N, keep, &dfi, &hi)))
+    if ((s = imp::out_device_staged(ctx, fhd_r, N, &dfr, &hr)) ||
+        (s = imp::out_device_staged(ctx, fhd_i, N, &dfi, &hi)))
         return s;
     IMP_CUDA(ts.compute_fhd(dkx, dky, dkz, dkr, dki, dfr, dfi), "F^H d gridding");
     if (hr && (s = copy_out(ctx, fhd_r, dfr, N))) return s;
@@ -1078,20 +1088,21 @@ static imp_status toeplitz_common(imp_context *ctx, const imp_toeplitz_options *
     if (num_coil <= 0 || (num_coil > 1 && (!sensi_r || !sensi_i)))
         return fail(IMP_ERR_INVALID_ARG, "num_coil > 0 and sensi for num_coil > 1");
     if ((s = imp::begin(ctx)) != IMP_OK) return s;
+    imp::stage_reset(ctx);
     const size_t N = (size_t)nx * ny * nz, C = num_coil;
     const float *dt, *dfm = nullptr, *dsr = nullptr, *dsi = nullptr, *dqr, *dqi;
-    if ((s = imp::to_device(ctx, t, num_k, keep, &dt, nullptr)) ||
-        (s = imp::to_device(ctx, fm, N, keep, &dfm, nullptr)) ||
-        (s = imp::to_device(ctx, num_coil > 1 ? sensi_r : nullptr, C * N, keep, &dsr, nullptr)) ||
-        (s = imp::to_device(ctx, num_coil > 1 ? sensi_i : nullptr, C * N, keep, &dsi, nullptr)))
+    if ((s = imp::to_device_staged(ctx, t, num_k, &dt, nullptr)) ||
+        (s = imp::to_device_staged(ctx, fm, N, &dfm, nullptr)) ||
+        (s = imp::to_device_staged(ctx, num_coil > 1 ? sensi_r : nullptr, C * N, &dsr, nullptr)) ||
+        (s = imp::to_device_staged(ctx, num_coil > 1 ? sensi_i : nullptr, C * N, &dsi, nullptr)))
         return s;
     imp::ToepSolver &ts = solver_of(ctx);
     IMP_CUDA(ts.setup(toep_cfg(opt, nx, ny, nz, num_coil, num_k), dt, dfm, dsr, dsi,
                       ctx->dev_err, ctx->stream),
              "toeplitz setup");
     const size_t nq = (size_t)ts.segments() * ts.q_elems();
-    if ((s = imp::to_device(ctx, q_r, nq, keep, &dqr, nullptr)) ||
-        (s = imp::to_device(ctx, q_i, nq, keep, &dqi, nullptr)))
+    if ((s = imp::to_device_staged(ctx, q_r, nq, &dqr, nullptr)) ||
+        (s = imp::to_device_staged(ctx, q_i, nq, &dqi, nullptr)))
         return s;
     IMP_CUDA(ts.load_q(dqr, dqi), "Qf");
     *out = &ts;
@@ -1113,10 +1124,10 @@ imp_status imp_toeplitz_recon(imp_context *ctx, const imp_toeplitz_options *opt,
     const float *dfr, *dfi;
     float *dxr, *dxi;
     bool hr, hi;
-    if ((s = imp::to_device(ctx, fhd_r, N, keep, &dfr, nullptr)) ||
-        (s = imp::to_device(ctx, fhd_i, N, keep, &dfi, nullptr)) ||
-        (s = imp::out_device(ctx, x_r, N, keep, &dxr, &hr)) ||
-        (s = imp::out_device(ctx, x_i, N, keep, &dxi, &hi)))
+    if ((s = imp::to_device_staged(ctx, fhd_r, N, &dfr, nullptr)) ||
+        (s = imp::to_device_staged(ctx, fhd_i, N, &dfi, nullptr)) ||
+        (s = imp::out_device_staged(ctx, x_r, N, &dxr, &hr)) ||
+        (s = imp::out_device_staged(ctx, x_i, N, &dxi, &hi)))
         return s;
     IMP_CUDA(ts->solve(dfr, dfi, dxr, dxi), "toeplitz CG");
     if (hr && (s = copy_out(ctx, x_r, dxr, N))) return s;
@@ -1144,12 +1155,12 @@ imp_status imp_toeplitz_cg(imp_context *ctx, const imp_toeplitz_options *opt, fl
     const float *dfr, *dfi, *dx0r, *dx0i;
     float *dxr, *dxi;
     bool hr, hi;
-    if ((s = imp::to_device(ctx, fhd_r, N, keep, &dfr, nullptr)) ||
-        (s = imp::to_device(ctx, fhd_i, N, keep, &dfi, nullptr)) ||
-        (s = imp::to_device(ctx, x_r, N, keep, &dx0r, nullptr)) ||
-        (s = imp::to_device(ctx, x_i, N, keep, &dx0i, nullptr)) ||
-        (s = imp::out_device(ctx, x_r, N, keep, &dxr, &hr)) ||
-        (s = imp::out_device(ctx, x_i, N, keep, &dxi, &hi)))
+    if ((s = imp::to_device_staged(ctx, fhd_r, N, &dfr, nullptr)) ||
+        (s = imp::to_device_staged(ctx, fhd_i, N, &dfi, nullptr)) ||
+        (s = imp::to_device_staged(ctx, x_r, N, &dx0r, nullptr)) ||
+        (s = imp::to_device_staged(ctx, x_i, N, &dx0i, nullptr)) ||
+        (s = imp::out_device_staged(ctx, x_r, N, &dxr, &hr)) ||
+        (s = imp::out_device_staged(ctx, x_i, N, &dxi, &hi)))
         return s;
     if (hr) IMP_CUDA(cudaMemcpyAsync(dxr, dx0r, N * 4, cudaMemcpyDeviceToDevice, ctx->stream), "x0");
     if (hi) IMP_CUDA(cudaMemcpyAsync(dxi, dx0i, N * 4, cudaMemcpyDeviceToDevice, ctx->stream), "x0");
@@ -1179,10 +1190,10 @@ imp_status imp_toeplitz_apply(imp_context *ctx, const imp_toeplitz_options *opt,
     const float *dpr, *dpi;
     float *dor, *doi;
     bool hr, hi;
-    if ((s = imp::to_device(ctx, p_r, N, keep, &dpr, nullptr)) ||
-        (s = imp::to_device(ctx, p_i, N, keep, &dpi, nullptr)) ||
-        (s = imp::out_device(ctx, q_out_r, N, keep, &dor, &hr)) ||
-        (s = imp::out_device(ctx, q_out_i, N, keep, &doi, &hi)))
+    if ((s = imp::to_device_staged(ctx, p_r, N, &dpr, nullptr)) ||
+        (s = imp::to_device_staged(ctx, p_i, N, &dpi, nullptr)) ||
+        (s = imp::out_device_staged(ctx, q_out_r, N, &dor, &hr)) ||
+        (s = imp::out_device_staged(ctx, q_out_i, N, &doi, &hi)))
         return s;
     IMP_CUDA(ts->apply(dpr, dpi, dor, doi), "toeplitz apply");
     if (hr && (s = copy_out(ctx, q_out_r, dor, N))) return s;
