@@ -43,33 +43,25 @@ UNIT = "s/recon"
 CG_NUM, TV_NUM, LAMBDA = 16, 10, 1e-3
 
 
+def _replicas():
+    from __graft_entry__ import load_package
+    load_package()
+    from impatient_mri_b200 import replicas
+    return replicas
+
+
 def dist_setup():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    return ws, rank, local
+    """One process per GPU (torchrun environment); NCCL process group for the
+    host-side barrier and the max-over-ranks timing only."""
+    return _replicas().init(timeout_s=300)
 
 
 def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    _replicas().barrier(ws)
 
 
 def max_over_ranks(v, ws):
-    if ws == 1:
-        return v
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return _replicas().max_over_ranks(v, ws)
 
 
 class ClockSampler:
@@ -634,23 +626,27 @@ BATCH_METRIC = ("s/recon (brute-force CG, 64 independent 2-D 384x384 slices, 32 
                 "16-32 x 4096-sample spirals per slice, 20 CG iterations)")
 
 
-def run_batch(args, local):
+def run_batch(args, ws, rank, local):
     """Configuration 4: independent 384x384 slices with 32 ring coils, each with
     its own seeded spiral of 16..32 interleaves x 4096 samples (uneven M), field
-    map and phantom; plain CG, cg_num 20 (19 updates).  All slices go through
-    one imp_bruteforce_batch call.  The timed job is the first `--slices`
-    slices of the seeded 64; value = its time scaled by the ratio of all 64
-    slices' sample counts to the timed slices' (extrapolated, stated in
-    config; the work per slice is proportional to its sample count)."""
+    map and phantom; plain CG, cg_num 20 (19 updates).  The timed job is the
+    first `--slices` slices of the seeded 64; with N GPUs each rank takes a
+    contiguous share of them (replicas, as the reference's -mgpu) through one
+    imp_bruteforce_batch call, and the job time is the maximum over ranks.
+    value = that time scaled by the ratio of all 64 slices' sample counts to
+    the timed slices' (1 when all 64 are timed; the work per slice is
+    proportional to its sample count)."""
     import torch
     from __graft_entry__ import load_package
     pkg = load_package()
     from impatient_mri_b200 import synth
+    R = _replicas()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     ctx = pkg.Context(local)
     n, C, S_total = 384, 32, 64
     S = max(1, min(args.slices, S_total))
+    lo, hi = R.slice_range(S, ws, rank)
     rng = np.random.default_rng(1004)
     ix, iy, iz = synth.grid_positions(n, n, 1)
     sens = np.stack([synth.to_voxel_order(m)
@@ -665,7 +661,7 @@ def run_batch(args, local):
         img = synth.to_voxel_order(synth.ellipse_phantom((n, n), 8, rng))
         fm = synth.to_voxel_order(synth.field_map((n, n), rng)).astype(np.float32)
         ms.append(skx.size)
-        if s_ >= S:
+        if not lo <= s_ < hi:
             continue
         M = skx.size
         yr = torch.zeros(C * M, device=dev)
@@ -674,18 +670,23 @@ def run_batch(args, local):
         pkg.parallelFtGpu(ctx, yr, yi, f(img.real), f(img.imag), g["kx"], g["ky"], g["kz"],
                           D["ix"], D["iy"], D["iz"], g["fm"], g["t"], M, N, D["sr"], D["si"], C, 0)
         y = yr.cpu().numpy() + 1j * yi.cpu().numpy()
-        y = synth.add_noise(y, 40.0, rng).astype(np.complex64)
+        # per-slice noise seed: the data do not depend on how slices are sharded
+        y = synth.add_noise(y, 40.0, np.random.default_rng(5000 + s_)).astype(np.complex64)
         kx.append(skx); ky.append(sky); tt.append(st); fms.append(fm)
         kdr.append(y.real.astype(np.float32)); kdi.append(y.imag.astype(np.float32))
-    k_off = np.cumsum([0] + ms[:S])
-    B = dict(kx=f(np.concatenate(kx)), ky=f(np.concatenate(ky)),
-             kz=f(np.zeros(int(k_off[-1]), np.float32)), t=f(np.concatenate(tt)),
-             fm=f(np.concatenate(fms)), kr=f(np.concatenate(kdr)), ki=f(np.concatenate(kdi)))
-    xr = torch.zeros(S * N, device=dev)
-    xi = torch.zeros(S * N, device=dev)
+    mine = hi - lo
+    if mine:
+        k_off = np.cumsum([0] + ms[lo:hi])
+        B = dict(kx=f(np.concatenate(kx)), ky=f(np.concatenate(ky)),
+                 kz=f(np.zeros(int(k_off[-1]), np.float32)), t=f(np.concatenate(tt)),
+                 fm=f(np.concatenate(fms)), kr=f(np.concatenate(kdr)), ki=f(np.concatenate(kdi)))
+    xr = torch.zeros(max(mine, 1) * N, device=dev)
+    xi = torch.zeros(max(mine, 1) * N, device=dev)
     opts = pkg.bf_options(cg_num=20)
 
     def recon():
+        if not mine:  # more ranks than timed slices: this rank has no work
+            return
         xr.zero_(); xi.zero_()
         pkg.bruteForceBatch(ctx, opts, xr, xi, B["kr"], B["ki"], B["kx"], B["ky"], B["kz"],
                             B["t"], k_off, D["ix"], D["iy"], D["iz"], B["fm"], D["sr"], D["si"],
@@ -697,31 +698,40 @@ def run_batch(args, local):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     launches = 0
+    barrier(ws)
+    torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         for s_ in range(args.steps):
             ev[s_][0].record()
             recon()
             ev[s_][1].record()
-            launches += ctx.launch_count()
+            launches += ctx.launch_count() if mine else 0
     torch.cuda.synchronize()
-    ms_step = float(np.mean([a.elapsed_time(b) for a, b in ev]))
+    barrier(ws)
+    # whole job: every rank's share of the timed slices, time = max over ranks
+    ms_step = max_over_ranks(float(np.mean([a.elapsed_time(b) for a, b in ev])), ws)
+    launches = int(round(max_over_ranks(float(launches), ws)))
     pairs = float(sum(ms[:S])) * N
     applies = 1 + 2 * 19
     flop = 2.0 * (3 + 4 * C) * pairs * applies
     achieved = flop / (ms_step / 1e3) / 1e12
     fp32_peak, _ = pkg.measure_alu_peaks(local)
     scale = float(sum(ms)) / float(sum(ms[:S]))  # work is proportional to the sample count
+    if rank != 0:
+        ctx.close()
+        return 0
     line = {
-        "metric": BATCH_METRIC, "value": ms_step / 1e3 * scale, "unit": UNIT, "n_gpus": 1,
+        "metric": BATCH_METRIC, "value": ms_step / 1e3 * scale, "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "higher_is_better": False, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded spirals, phantoms, field maps, ring coils; 40 dB noise)",
         "config": {"workload": f"{BATCH}: {S} of 64 slices timed (sample counts "
                                f"{ms[:S]}); value = that time x {scale:.2f} (all 64 slices' "
                                f"samples / the timed slices' samples); 384x384, 32 coils, "
                                f"cg_num 20, no regularization",
-                   "parallelism": "one imp_bruteforce_batch call: all slices in lockstep, "
-                                  "one launch per CG step over every slice"},
+                   "parallelism": f"replicas x{ws}: each GPU one imp_bruteforce_batch call "
+                                  "over its contiguous share of the slices (all its slices "
+                                  "in lockstep, one launch per CG step)"},
         "gpu_launches": launches,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                      "frac": achieved / fp32_peak, "traffic": None,
@@ -955,12 +965,10 @@ def main() -> int:
         if args.workload == WARM:
             return run_warm(args, local)
         if args.workload == BATCH:
-            return run_batch(args, local)
+            return run_batch(args, ws, rank, local)
         return run_ours(args, ws, rank, local)
     finally:
-        if ws > 1:
-            import torch.distributed as dist
-            dist.destroy_process_group()
+        _replicas().finalize(ws)
 
 
 if __name__ == "__main__":
