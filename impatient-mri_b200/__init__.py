@@ -40,7 +40,7 @@ EXPORTED = [
     "imp_context_launch_count", "imp_context_profile", "imp_context_profile_read",
     "imp_ft", "imp_ift", "imp_parallel_ft", "imp_parallel_ift", "imp_parallel_ift_noalloc",
     "imp_bf_options_default", "imp_bruteforce_recon", "imp_bruteforce_dir",
-    "imp_bruteforce_batch",
+    "imp_bruteforce_batch", "imp_bruteforce_mgpu",
     "imp_dataset_info", "imp_mrisolver_main", "imp_measure_alu_peaks",
     "imp_toeplitz_options_default", "imp_toeplitz_q", "imp_toeplitz_fhd", "imp_toeplitz_recon",
     "imp_toeplitz_apply", "imp_toeplitz_dir", "imp_toeplitz_cg",
@@ -107,6 +107,8 @@ def lib() -> ctypes.CDLL:
                                            + [ip, ip, ip, ip])
         L.imp_bruteforce_batch.argtypes = ([vp, ctypes.POINTER(BfOptions)] + [vp] * 8
                                            + [ctypes.POINTER(ip)] + [vp] * 6 + [ip, ip, ip])
+        L.imp_bruteforce_mgpu.argtypes = ([ctypes.POINTER(BfOptions)] + [vp] * 14
+                                          + [ip, ip, ip, ip, ctypes.POINTER(ip), ip])
         L.imp_bruteforce_dir.argtypes = [ctypes.c_char_p, ctypes.c_char_p,
                                          ctypes.POINTER(BfOptions), ip]
         L.imp_dataset_info.argtypes = [ctypes.c_char_p] + [ctypes.POINTER(ctypes.c_int)] * 7
@@ -269,6 +271,23 @@ def bruteForceBatch(ctx, opts: BfOptions, idata_r, idata_i, kdata_r, kdata_i, kx
         ctx.handle, ctypes.byref(opts), *map(_ptr, (idata_r, idata_i, kdata_r, kdata_i, kx, ky,
                                                     kz, t)),
         off, *map(_ptr, (ix, iy, iz, fm, sensi_r, sensi_i)), num_i, num_coil, len(k_off) - 1))
+
+
+def bruteForceMgpu(opts: BfOptions, idata_r, idata_i, kdata_r, kdata_i, kx, ky, kz, ix, iy,
+                   iz, fm, t, sensi_r, sensi_i, num_k, num_i, num_coil, num_slices,
+                   devices=None) -> None:
+    """-mgpu: the slices of bruteForceGpu spread over GPUs, one worker thread
+    and context per entry of `devices` (None: every visible GPU).  Host
+    arrays; idata_* receive the images."""
+    dev = None
+    n = 0
+    if devices is not None:
+        dev = (ctypes.c_int * len(devices))(*[int(d) for d in devices])
+        n = len(devices)
+    _check(lib().imp_bruteforce_mgpu(
+        ctypes.byref(opts), *map(_ptr, (idata_r, idata_i, kdata_r, kdata_i, kx, ky, kz, ix, iy,
+                                        iz, fm, t, sensi_r, sensi_i)),
+        num_k, num_i, num_coil, num_slices, dev, n))
 
 
 def bruteForce(idir: str, odir: str, opts: BfOptions, gpu_id: int = 0) -> None:

@@ -1,13 +1,20 @@
 // mriSolver command line (flags, defaults and messages of main.cpp:96-444)
 // and the directory-level drop-in of bruteForce() (main_mri.cu:652-1025).
 #include "../../include/impatient_b200.h"
+#include "context.h"
 #include "io.h"
 
+#include <cuda_runtime.h>
+
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <thread>
+#include <vector>
 
 namespace {
 
@@ -27,11 +34,68 @@ void usage(FILE *f) {
                  "  -reuseQ <dir>, -writeQ reuse / write Q_stone.file (Toeplitz)\n"
                  "  -gpu_id <id>           CUDA device (default 0)\n"
                  "  -bf3d                  brute force with the true 3-D phase and 3-D TV\n"
-                 "  -mgpu                  accepted; slices run on one GPU\n"
+                 "  -mgpu                  slices spread over every visible GPU (brute force)\n"
                  "  -cpu, -nogpu, -reg     not provided by this build\n");
 }
 
 }  // namespace
+
+// Work queue of the -mgpu path (bruteForceMgpu, bruteForce/bruteForceMgpu.cu:82,
+// started per GPU at main_mri.cu:900; the reference splits the slices into
+// contiguous blocks per GPU, main_mri.cu:776-834).  Here every worker thread
+// owns one context on its device and claims slices from a shared counter, so
+// uneven slices balance; each slice is one imp_bruteforce_recon call on the
+// slice's views of the host arrays.
+extern "C" imp_status imp_bruteforce_mgpu(const imp_bf_options *opt, float *idata_r,
+                                          float *idata_i, const float *kdata_r,
+                                          const float *kdata_i, const float *kx,
+                                          const float *ky, const float *kz, const float *ix,
+                                          const float *iy, const float *iz, const float *fm,
+                                          const float *t, const float *sensi_r,
+                                          const float *sensi_i, int num_k, int num_i,
+                                          int num_coil, int num_slices, const int *devices,
+                                          int num_workers) {
+    if (!opt || !idata_r || !idata_i || !kdata_r || !kdata_i || num_slices <= 0 ||
+        num_k <= 0 || num_i <= 0 || num_coil <= 0)
+        return IMP_ERR_INVALID_ARG;
+    if (num_workers <= 0) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0)
+            return imp::fail(IMP_ERR_CUDA, "no CUDA device for -mgpu");
+        num_workers = n;
+    }
+    num_workers = std::min(num_workers, num_slices);
+    const size_t N = (size_t)num_i, KC = (size_t)num_k * num_coil;
+    std::atomic<int> next{0};
+    std::atomic<int> failed{IMP_OK};
+    std::mutex mu;
+    std::string first_msg;
+    auto worker = [&](int w) {
+        const int dev = devices ? devices[w] : w;
+        imp_context *ctx = nullptr;
+        imp_status s = imp_context_create(dev, &ctx);
+        while (s == IMP_OK && failed.load() == IMP_OK) {
+            const int sl = next.fetch_add(1);
+            if (sl >= num_slices) break;
+            s = imp_bruteforce_recon(ctx, opt, idata_r + sl * N, idata_i + sl * N,
+                                     kdata_r + sl * KC, kdata_i + sl * KC, kx, ky, kz, ix, iy,
+                                     iz, fm ? fm + sl * N : nullptr, t, sensi_r, sensi_i, num_k,
+                                     num_i, num_coil, 1);
+        }
+        if (s != IMP_OK) {
+            std::lock_guard<std::mutex> lk(mu);
+            int expect = IMP_OK;
+            if (failed.compare_exchange_strong(expect, s))
+                first_msg = "GPU " + std::to_string(dev) + ": " + imp_last_error();
+        }
+        imp_context_destroy(ctx);
+    };
+    std::vector<std::thread> pool;
+    for (int w = 0; w < num_workers; ++w) pool.emplace_back(worker, w);
+    for (std::thread &th : pool) th.join();
+    const int s = failed.load();
+    return s == IMP_OK ? IMP_OK : imp::fail((imp_status)s, first_msg);  // message in this thread
+}
 
 extern "C" imp_status imp_bruteforce_dir(const char *idir, const char *odir,
                                          const imp_bf_options *opt, int gpu_id) {
@@ -63,18 +127,30 @@ extern "C" imp_status imp_bruteforce_dir(const char *idir, const char *odir,
     std::printf("  Number of CG iterations: %d\n", o.cg_num);
     if (o.enable_fd) std::printf("  FD penalizer value     : %f\n", o.fd_penalizer);
     if (o.enable_tv) std::printf("  Number of TV iterations: %d\n", o.tv_num);
-    imp_context *ctx = nullptr;
-    st = imp_context_create(gpu_id, &ctx);
-    if (st != IMP_OK) {
-        std::fprintf(stderr, "Error: %s\n", imp_last_error());
-        return st;
+    if (gpu_id < 0) {  // -mgpu
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) n = 0;
+        std::printf("  Number of online GPUs  : %d\n", n);
+        st = imp_bruteforce_mgpu(&o, ds.idata_r.data(), ds.idata_i.data(), ds.kdata_r.data(),
+                                 ds.kdata_i.data(), ds.kx.data(), ds.ky.data(), ds.kz.data(),
+                                 ds.ix.data(), ds.iy.data(), ds.iz.data(), ds.fm.data(),
+                                 ds.t.data(), ds.sensi_r.data(), ds.sensi_i.data(), ds.num_k,
+                                 ds.num_i, ds.num_coil, ds.num_slices, nullptr, 0);
+    } else {
+        imp_context *ctx = nullptr;
+        st = imp_context_create(gpu_id, &ctx);
+        if (st != IMP_OK) {
+            std::fprintf(stderr, "Error: %s\n", imp_last_error());
+            return st;
+        }
+        st = imp_bruteforce_recon(ctx, &o, ds.idata_r.data(), ds.idata_i.data(),
+                                  ds.kdata_r.data(), ds.kdata_i.data(), ds.kx.data(),
+                                  ds.ky.data(), ds.kz.data(), ds.ix.data(), ds.iy.data(),
+                                  ds.iz.data(), ds.fm.data(), ds.t.data(), ds.sensi_r.data(),
+                                  ds.sensi_i.data(), ds.num_k, ds.num_i, ds.num_coil,
+                                  ds.num_slices);
+        imp_context_destroy(ctx);
     }
-    st = imp_bruteforce_recon(ctx, &o, ds.idata_r.data(), ds.idata_i.data(), ds.kdata_r.data(),
-                              ds.kdata_i.data(), ds.kx.data(), ds.ky.data(), ds.kz.data(),
-                              ds.ix.data(), ds.iy.data(), ds.iz.data(), ds.fm.data(),
-                              ds.t.data(), ds.sensi_r.data(), ds.sensi_i.data(), ds.num_k,
-                              ds.num_i, ds.num_coil, ds.num_slices);
-    imp_context_destroy(ctx);
     if (st != IMP_OK) {
         std::fprintf(stderr, "Error: %s\n", imp_last_error());
         return st;
@@ -254,7 +330,9 @@ extern "C" int imp_mrisolver_main(int argc, char **argv) {
         std::fprintf(stderr, "\nError: -cpu / -nogpu: this build has no CPU reconstruction path.\n");
         return 1;
     }
-    if (mgpu) std::printf("mriSolver: -mgpu: all slices run on GPU %d.\n", gpu_id);
+    if (mgpu && (tgrid || tdirect))
+        std::printf("mriSolver: -mgpu applies to the brute-force path; Toeplitz runs on GPU %d.\n",
+                    gpu_id);
     imp_status st;
     if (tgrid || tdirect) {
         st = imp_toeplitz_dir_cli(idir.c_str(), odir.c_str(), cg_num, fd, fdp, tv, tv_num,
@@ -269,7 +347,7 @@ extern "C" int imp_mrisolver_main(int argc, char **argv) {
         o.enable_tv = tv;
         o.tv_num = tv_num;
         o.use_z = bf3d;
-        st = imp_bruteforce_dir(idir.c_str(), odir.c_str(), &o, gpu_id);
+        st = imp_bruteforce_dir(idir.c_str(), odir.c_str(), &o, mgpu ? -1 : gpu_id);
     }
     if (st != IMP_OK) {
         std::fprintf(stderr, "Error: Failed to execute the mriSolver.\n");

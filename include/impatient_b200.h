@@ -159,6 +159,22 @@ imp_status imp_bruteforce_recon(imp_context *ctx, const imp_bf_options *opt, flo
                                 const float *sensi_i, int num_k, int num_i, int num_coil,
                                 int num_slices);
 
+/* The slices of imp_bruteforce_recon spread over several GPUs: one host
+ * thread per worker, each with its own context on devices[w] (devices null:
+ * GPUs 0 .. num_workers-1; num_workers <= 0: every visible GPU), takes the
+ * next unclaimed slice and reconstructs it; images land in disjoint slices of
+ * idata.  Host arrays, same layouts as imp_bruteforce_recon.  The first failure
+ * stops further slices and is returned.
+ * replaces the -mgpu path: bruteForceMgpu / its pthread work queue,
+ * bruteForce/bruteForceMgpu.cu:81-128, main_mri.cu:770-834 */
+imp_status imp_bruteforce_mgpu(const imp_bf_options *opt, float *idata_r, float *idata_i,
+                               const float *kdata_r, const float *kdata_i, const float *kx,
+                               const float *ky, const float *kz, const float *ix,
+                               const float *iy, const float *iz, const float *fm,
+                               const float *t, const float *sensi_r, const float *sensi_i,
+                               int num_k, int num_i, int num_coil, int num_slices,
+                               const int *devices, int num_workers);
+
 /* Brute-force CG recon of num_slices slices that share the image grid
  * (ix, iy, iz: num_i) and the coil maps but each have their own trajectory and
  * sample count (uneven M), k-space data and field map -- the multi-slice loop
@@ -181,7 +197,8 @@ imp_status imp_bruteforce_batch(imp_context *ctx, const imp_bf_options *opt, flo
  * main_mri.cu:652-1025): reads idir in the 0.2 or 1.0 format
  * (kernels/structures.cpp:569-1162), reconstructs every slice and writes
  * odir/output_gpu_r.dat and odir/output_gpu_i.dat as "%f\n" text
- * (kernels/structures.cpp:1165-1175). */
+ * (kernels/structures.cpp:1165-1175).  gpu_id < 0 is the -mgpu mode: the
+ * slices are spread over every visible GPU (imp_bruteforce_mgpu). */
 imp_status imp_bruteforce_dir(const char *idir, const char *odir, const imp_bf_options *opt,
                               int gpu_id);
 

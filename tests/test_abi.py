@@ -40,6 +40,17 @@ def test_context_create_without_gpu_fails_cleanly(pkg):
     assert e.value.status in (1, 2)
 
 
+@pytest.mark.skipif(has_cuda(), reason="checks the no-GPU error path")
+def test_mgpu_without_gpu_fails_cleanly(pkg):
+    """-mgpu with no visible GPU: an error status and message, no worker runs."""
+    import numpy as np
+    a = np.zeros(16, np.float32)
+    with pytest.raises(pkg.ImpError) as e:
+        pkg.bruteForceMgpu(pkg.bf_options(cg_num=2), a, a, a, a, a, a, a, a, a, a, a, a, a, a,
+                           16, 16, 1, 1)
+    assert e.value.status == 2 and "device" in str(e.value)
+
+
 def test_invalid_device_is_rejected(pkg):
     with pytest.raises(pkg.ImpError):
         pkg.Context(9999)

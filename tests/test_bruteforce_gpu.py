@@ -120,6 +120,58 @@ def test_multi_slice_equals_slice_by_slice(pkg, ctx):
     assert np.array_equal(x[:N], a) and np.array_equal(x[N:], b)
 
 
+def _mgpu_case(n_slices):
+    c = golden("bf_2d_c3")
+    rng = np.random.default_rng(3)
+    kds, fms = [], []
+    for s in range(n_slices):
+        kds.append(c["kdata"] * (0.4 + 0.15 * s + 0.1j)
+                   + 0.01 * rng.standard_normal(c["kdata"].shape))
+        fms.append((c["fm"] * (1.0 - 0.3 * s)).astype(np.float32))
+    return c, np.concatenate([k.ravel() for k in kds]), np.concatenate(fms)
+
+
+def _mgpu_args(c, kd, fm, n_slices):
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    N, M = c["ix"].size, c["kx"].size
+    C = np.asarray(c["sens"]).size // N
+    s = np.asarray(c["sens"]).reshape(C, N)
+    xr, xi = np.zeros(n_slices * N, np.float32), np.zeros(n_slices * N, np.float32)
+    args = (xr, xi, f32(kd.real), f32(kd.imag), f32(c["kx"]), f32(c["ky"]), f32(c["kz"]),
+            f32(c["ix"]), f32(c["iy"]), f32(c["iz"]), f32(fm), f32(c["t"]), f32(s.real),
+            f32(s.imag), M, N, C, n_slices)
+    return args, xr, xi
+
+
+def test_mgpu_work_queue_matches_one_context(pkg, ctx):
+    """-mgpu work queue: three worker threads, each with its own context on GPU
+    0, claim five slices; every slice equals the multi-slice call on one
+    context to 1e-5 (the contexts tune their launch shapes independently)."""
+    S = 5
+    c, kd, fm = _mgpu_case(S)
+    opts = pkg.bf_options(cg_num=5, fd_penalizer=1e-2, tv=True, tv_num=2)
+    args, xr, xi = _mgpu_args(c, kd, fm, S)
+    pkg.bruteForceMgpu(opts, *args, devices=[0, 0, 0])
+    got = xr + 1j * xi.astype(np.float64)
+    args1, yr, yi = _mgpu_args(c, kd, fm, S)
+    pkg.bruteForceGpu(ctx, opts, *args1)
+    ref = yr + 1j * yi.astype(np.float64)
+    N = c["ix"].size
+    for s in range(S):
+        assert oracle.rel_l2(got[s * N:(s + 1) * N], ref[s * N:(s + 1) * N]) < 1e-5, s
+
+
+def test_mgpu_reports_a_failing_worker(pkg):
+    """A worker whose device does not exist stops the queue; the call returns
+    its error (status and message) in the caller's thread."""
+    c, kd, fm = _mgpu_case(3)
+    opts = pkg.bf_options(cg_num=3)
+    args, _, _ = _mgpu_args(c, kd, fm, 3)
+    with pytest.raises(pkg.ImpError) as e:
+        pkg.bruteForceMgpu(opts, *args, devices=[0, 4096])
+    assert e.value.status == 1 and "4096" in str(e.value)
+
+
 def test_warm_start_from_idata(pkg, ctx):
     """idata is the initial estimate (bruteForceCpu starts from *idata)."""
     from gpu_util import gpu_recon
@@ -145,6 +197,27 @@ def test_cli_end_to_end(pkg, tmp_path):
     ref = oracle.bf_cg(c, cg_num=3, lam=1e-2, tv=True, tv_num=2, eps=1e-6, use_z=0)
     # "%f" keeps 6 decimals
     assert np.max(np.abs(xr + 1j * xi - ref)) < 1e-5 + 1e-4 * np.max(np.abs(ref))
+
+
+def test_cli_mgpu_matches_single_gpu(pkg, tmp_path):
+    """mriSolver -mgpu (slices over every visible GPU) writes the images of the
+    single-GPU run on a two-slice 0.2-format directory."""
+    from impatient_mri_b200 import io
+    c, kd, fm = _mgpu_case(2)
+    N = c["ix"].size
+    n = int(round(np.sqrt(N)))
+    io.write_dataset(tmp_path / "in", "0.2", kx=c["kx"], ky=c["ky"], kz=c["kz"], t=c["t"],
+                     ix=c["ix"], iy=c["iy"], iz=c["iz"], fm=fm, kdata=kd, sensi=c["sens"],
+                     dims=(n, n, 1), num_coil=np.asarray(c["sens"]).size // N, num_slices=2)
+    outs = []
+    for extra in ([], ["-mgpu"]):
+        od = tmp_path / ("out_m" if extra else "out_1")
+        rc = pkg.mriSolver("-idir", str(tmp_path / "in"), "-odir", str(od), "-cg_num", "3",
+                           "-fdp", "0.01", *extra)
+        assert rc == 0
+        outs.append(np.loadtxt(od / "output_gpu_r.dat") + 1j * np.loadtxt(od / "output_gpu_i.dat"))
+    assert outs[0].size == 2 * c["ix"].size
+    assert np.max(np.abs(outs[0] - outs[1])) <= 2e-6 + 1e-5 * np.max(np.abs(outs[0]))
 
 
 def test_batch_with_uneven_trajectories(pkg, ctx, synth):
