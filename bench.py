@@ -337,6 +337,139 @@ def run_ours(args, ws, rank, local):
     return 0
 
 
+# ------------------------------------------------------------------- C1 --
+
+C1 = "bf2d_64"
+C1_METRIC = "s/recon (brute-force 2-D CG, 64x64, 1 coil, M=4096, 8 CG x 10 TV)"
+
+
+def run_bf2d(args, ws, rank, local):
+    """Configuration 1, the reference's CPU-runnable case: 2-D 64x64, one coil,
+    4 x 1024 spiral (M = 4096), field map, TV lambda 1e-3 with 10 reweighting
+    passes (the reference's -tv default) of 8 CG iterations.  Data: this
+    library's exact-phase NUDFT of the seeded phantom + 40 dB noise.  The CPU
+    baseline is the reference's own bruteForceCpu (FP32 build; 1 thread and the
+    OpenMP build on all threads), full runs."""
+    import torch
+    from __graft_entry__ import load_package
+    pkg = load_package()
+    from impatient_mri_b200 import synth
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    ctx = pkg.Context(local)
+    case = synth.make_case(C1, seed=1001 + rank)
+    M, N = case["M"], case["N"]
+    f32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32))
+    D = {k: f32(case[k]).to(dev) for k in ("kx", "ky", "kz", "t", "ix", "iy", "iz", "fm")}
+    D["sr"], D["si"] = f32(case["sens"].real).to(dev), f32(case["sens"].imag).to(dev)
+    yr, yi = torch.zeros(M, device=dev), torch.zeros(M, device=dev)
+    pkg.parallelFtGpu(ctx, yr, yi, f32(case["x_true"].real).to(dev),
+                      f32(case["x_true"].imag).to(dev), D["kx"], D["ky"], D["kz"], D["ix"],
+                      D["iy"], D["iz"], D["fm"], D["t"], M, N, D["sr"], D["si"], 1, 0)
+    y = yr.cpu().numpy() + 1j * yi.cpu().numpy()
+    y = synth.add_noise(y, 40.0, np.random.default_rng(11 + rank)).astype(np.complex64)
+    D["yr"], D["yi"] = f32(y.real).to(dev), f32(y.imag).to(dev)
+    o = case["opts"]
+    opts = pkg.bf_options(cg_num=o["cg_num"], fd_penalizer=o["fd_penalizer"], tv=True,
+                          tv_num=o["tv_num"], tv_eps=1e-6)
+
+    def recon(x_r, x_i, s):
+        pkg.bruteForceGpu(ctx, opts, x_r, x_i, s["yr"], s["yi"], s["kx"], s["ky"], s["kz"],
+                          s["ix"], s["iy"], s["iz"], s["fm"], s["t"], s["sr"], s["si"], M, N, 1,
+                          1)
+
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    xr, xi = torch.zeros(N, device=dev), torch.zeros(N, device=dev)
+    for _ in range(max(args.warmup, 1)):
+        xr.zero_(); xi.zero_()
+        recon(xr, xi, D)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    launches = 0
+    barrier(ws)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            xr.zero_(); xi.zero_()
+            flush.fill_(float(s))
+            ev[s][0].record()
+            recon(xr, xi, D)
+            ev[s][1].record()
+            launches += ctx.launch_count()
+    torch.cuda.synchronize()
+    barrier(ws)
+    value = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev) / 1e3, ws) / (args.steps * ws)
+    H = {k: v.cpu().pin_memory() for k, v in D.items()}
+    hxr, hxi = torch.zeros(N).pin_memory(), torch.zeros(N).pin_memory()
+    h2d = sum(v.numel() * 4 for v in H.values()) + 2 * N * 4
+    recon(hxr, hxi, H)
+    e2e = []
+    for s in range(args.steps):
+        hxr.zero_(); hxi.zero_()
+        flush.fill_(float(s))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        recon(hxr, hxi, H)
+        e2e.append(time.perf_counter() - t0)
+    e2e_value = max_over_ranks(float(sum(e2e)), ws) / (args.steps * ws)
+    ctx.profile(True)
+    xr.zero_(); xi.zero_()
+    recon(xr, xi, D)
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    fwd_ms, fwd_n = prof["forward"]
+    adj_ms, adj_n = prof["adjoint"]
+    avg_launch_s = (fwd_ms + adj_ms) / max(fwd_n + adj_n, 1) / 1e3
+    fp32_peak, sfu_peak = pkg.measure_alu_peaks(local)
+    # one coil, 2-D phase: 2 MUFU per pair bound the NUDFT (14 FLOP per pair)
+    sfu_gops = 2.0 * M * N / avg_launch_s / 1e9
+    out = {
+        "metric": C1_METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": value * 1e3 * ws, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{C1}: 64x64, 1 coil, 4 x 1024 spiral (M=4096), field map, "
+                               f"cg_num 8, TV 10 passes, lambda 1e-3",
+                   "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": f"replicas x{ws}"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 2 * N * 4},
+        "gpu_launches": launches,
+        "roofline": {"bound": "sfu", "achieved": sfu_gops, "peak": sfu_peak, "unit": "Gop/s",
+                     "frac": sfu_gops / sfu_peak, "traffic": None,
+                     "kernel": "k_nudft (forward + adjoint): 2 MUFU (sin, cos) per pair",
+                     "peak_source": "measured MUFU throughput kernel (imp_measure_alu_peaks)",
+                     "avg_launch_ms": avg_launch_s * 1e3, "launches": fwd_n + adj_n,
+                     "share_of_recon": (fwd_ms + adj_ms) / 1e3 / value if value > 0 else None},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            import oracle
+            cpu_case = dict(case, kdata=y.astype(np.complex64))
+            runs = {}
+            for kind in ("bf32", "bf32_omp"):
+                if oracle.ref_available(kind):
+                    t0 = time.perf_counter()
+                    oracle.ref_bf_cg(cpu_case, kind=kind, cg_num=o["cg_num"],
+                                     lam=o["fd_penalizer"], tv=True, tv_num=o["tv_num"])
+                    runs[kind] = time.perf_counter() - t0
+            if "bf32_omp" in runs:
+                out["cpu_baseline"] = {
+                    "value": runs["bf32_omp"], "unit": UNIT, "cores": os.cpu_count(),
+                    "kind": "reference",
+                    "sample": ("reference bruteForceCpu FP32, full recon: OpenMP on all threads "
+                               f"{runs['bf32_omp']:.2f} s, one thread "
+                               f"{runs.get('bf32', float('nan')):.2f} s")}
+        except Exception as e:  # the baseline is reported, never required
+            out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(),
+                                   "kind": "reference", "sample": f"failed: {e}"}
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
 # ------------------------------------------------------------- Toeplitz --
 
 TOEP = "toep3d_256x256x32"
@@ -935,9 +1068,10 @@ def main() -> int:
     ap.add_argument("--ref-timeout", type=int, default=1200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--slices", type=int, default=4, help="batch384: slices timed")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, TOEP, WARM, BATCH],
-                    help="bf3d_64x64x16 (default, the headline), the Toeplitz 3-D case, or "
-                         "the learned warm start at 512x512 with 32 coils")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, C1, TOEP, WARM, BATCH],
+                    help="bf3d_64x64x16 (default, the headline), bf2d_64 (the 2-D one-coil "
+                         "case), the Toeplitz 3-D case, the learned warm start at 512x512 "
+                         "with 32 coils, or the 64-slice 384x384 batch")
     ap.add_argument("--retrain", action="store_true", help="warm512: train even if weights exist")
     ap.add_argument("--save-weights", default=None, help="warm512: where to write trained weights")
     ap.add_argument("--train-images", type=int, default=2000)
@@ -962,6 +1096,8 @@ def main() -> int:
             return run_reference(args, ws, rank)
         if args.workload == TOEP:
             return run_toeplitz(args, ws, rank, local)
+        if args.workload == C1:
+            return run_bf2d(args, ws, rank, local)
         if args.workload == WARM:
             return run_warm(args, local)
         if args.workload == BATCH:

@@ -14,6 +14,7 @@
 #include "context.h"
 #include "io.h"
 
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -200,8 +201,17 @@ extern "C" imp_status imp_toeplitz_dir(const char *idir, const imp_toeplitz_opti
     const float *kz = ds.kz.data();
     const float *fm = ds.fm.data();
     const float *sr = ds.sensi_r.data(), *si = ds.sensi_i.data();
+    // Q of the gridding path stays in device memory between steps 1 and 3
+    // (a host copy only for -writeQ); the other paths produce it on the host.
+    float *dq = nullptr;
+    const float *q_r = nullptr, *q_i = nullptr;
+    using clk = std::chrono::steady_clock;
+    auto ms_since = [](clk::time_point a) {
+        return std::chrono::duration<double, std::milli>(clk::now() - a).count();
+    };
     do {
         std::printf("======== Step 1. Compute Q matrices: Q[%d] ========\n", L + 1);
+        const auto tq = clk::now();
         if (reuseQ) {
             std::string qdir = Qdir ? Qdir : dir;
             std::printf("  Re-using the Q at %s/Q_stone.file\n", qdir.c_str());
@@ -209,16 +219,42 @@ extern "C" imp_status imp_toeplitz_dir(const char *idir, const imp_toeplitz_opti
         } else if (direct) {
             if ((st = direct_q(ctx, ds, Nx, Ny, Nz, L, tau, t0, qr, qi)) != IMP_OK) break;
         } else {
-            qr.resize(G * (L + 1));
-            qi.resize(G * (L + 1));
-            if ((st = imp_toeplitz_q(ctx, opt, qr.data(), qi.data(), ds.kx.data(), ds.ky.data(),
-                                     kz, ds.t.data(), ds.num_k, Nx, Ny, Nz)) != IMP_OK)
+            const size_t nq = G * (L + 1);
+            if (cudaSetDevice(gpu_id) != cudaSuccess ||
+                cudaMalloc(&dq, 2 * nq * sizeof(float)) != cudaSuccess) {
+                std::fprintf(stderr, "Error: no device memory for Q (%zu bytes)\n",
+                             2 * nq * sizeof(float));
+                st = IMP_ERR_NOMEM;
                 break;
+            }
+            if ((st = imp_toeplitz_q(ctx, opt, dq, dq + nq, ds.kx.data(), ds.ky.data(), kz,
+                                     ds.t.data(), ds.num_k, Nx, Ny, Nz)) != IMP_OK)
+                break;
+            q_r = dq;
+            q_i = dq + nq;
+            if (writeQ) {
+                qr.resize(nq);
+                qi.resize(nq);
+                if (cudaMemcpy(qr.data(), q_r, nq * sizeof(float), cudaMemcpyDeviceToHost) !=
+                        cudaSuccess ||
+                    cudaMemcpy(qi.data(), q_i, nq * sizeof(float), cudaMemcpyDeviceToHost) !=
+                        cudaSuccess) {
+                    std::fprintf(stderr, "Error: Q device-to-host copy failed\n");
+                    st = IMP_ERR_CUDA;
+                    break;
+                }
+            }
         }
+        if (!q_r) {
+            q_r = qr.data();
+            q_i = qi.data();
+        }
+        std::printf("  GPU: Q Kernel Time: %f (ms)\n", ms_since(tq));
         if (writeQ && !reuseQ &&
             (st = write_pairs(dir + "/Q_stone.file", qr, qi, G, L + 1)) != IMP_OK)
             break;
         std::printf("======== Step 2. Compute FH ========\n");
+        const auto tf = clk::now();
         if (direct) {
             if ((st = direct_fhd(ctx, ds, Nz > 1, fr, fi)) != IMP_OK) break;
         } else if ((st = imp_toeplitz_fhd(ctx, opt, fr.data(), fi.data(), ds.kdata_r.data(),
@@ -226,17 +262,21 @@ extern "C" imp_status imp_toeplitz_dir(const char *idir, const imp_toeplitz_opti
                                           ds.t.data(), fm, sr, si, ds.num_k, ds.num_coil, Nx,
                                           Ny, Nz)) != IMP_OK)
             break;
+        std::printf("  GPU: F^H(d) Kernel Time: %f (ms)\n", ms_since(tf));
         if ((st = write_pairs(dir + "/FhD.file", fr, fi, N, 1)) != IMP_OK) break;
         std::printf("======== Step 3. Toeplitz CG ========\n");
-        if ((st = imp_toeplitz_recon(ctx, opt, xr.data(), xi.data(), fr.data(), fi.data(),
-                                     qr.data(), qi.data(), ds.t.data(), ds.num_k, fm, sr, si,
-                                     ds.num_coil, Nx, Ny, Nz)) != IMP_OK)
+        const auto tc = clk::now();
+        if ((st = imp_toeplitz_recon(ctx, opt, xr.data(), xi.data(), fr.data(), fi.data(), q_r,
+                                     q_i, ds.t.data(), ds.num_k, fm, sr, si, ds.num_coil, Nx,
+                                     Ny, Nz)) != IMP_OK)
             break;
+        std::printf("  GPU: CG Execution Time: %f (ms)\n", ms_since(tc));
         if ((st = write_pairs(dir + "/out.file", xr, xi, N, 1)) != IMP_OK) break;
         std::printf("  GPU: Exporting results to %s/out.file\n", idir);
     } while (false);
     if (st != IMP_OK && st != IMP_ERR_IO && st != IMP_ERR_FORMAT)
         std::fprintf(stderr, "Error: %s\n", imp_last_error());
+    if (dq) cudaFree(dq);
     imp_context_destroy(ctx);
     return st;
 }
