@@ -615,10 +615,13 @@ __device__ __forceinline__ TcTile tc_tile(int t, int n_nt, int tiles_x, int tile
 // vector group to the BF16 output (at the pixel, or with up2 at the 2 x 2
 // block of the pixel in an image of twice the size: nearest up-sampling)
 // and / or the FP32 output (optionally accumulated).
-template <int NT>
+// STRIP: the tile is 128 consecutive pixels of one image row (x0 .. x0+127
+// of row y0) instead of an 8 x 16 patch.
+template <int NT, bool STRIP = false>
 __device__ __forceinline__ void conv_tc_store(const ConvArgs &a, const TcTile &T, uint32_t tacc,
                                               int r) {
-    const int xx = T.x0 + (r & (kTileX - 1)), yy = T.y0 + r / kTileX;
+    const int xx = STRIP ? T.x0 + r : T.x0 + (r & (kTileX - 1));
+    const int yy = STRIP ? T.y0 : T.y0 + r / kTileX;
     const bool valid = xx < a.W && yy < a.H;
     const size_t p = ((size_t)T.b * a.H + yy) * a.W + xx;
 #pragma unroll 1
@@ -905,12 +908,15 @@ cudaError_t conv_tc_n(const ConvArgs &a, unsigned *err, cudaStream_t st) {
 // The tensor-memory path for a convolution: channel counts multiples of 16,
 // channel strides and offsets multiples of 16 (16-byte aligned TMA rows and
 // vector stores).
+bool conv_args_ok(const ConvArgs &a) {
+    return !(a.cin % 16 || a.cout % 16 || a.ldx % 16 || a.xoff % 16 || a.xoff + a.cin > a.ldx ||
+             (a.y && (a.ldy % 16 || a.yoff % 16 || a.yoff + a.cout > a.ldy)) ||
+             (a.yf && (a.ldyf % 16 || a.yfoff % 16 || a.yfoff + a.cout > a.ldyf)) ||
+             (a.ks != 1 && a.ks != 3) || a.B < 1 || a.H < 1 || a.W < 1 || (a.up2 && !a.y));
+}
+
 cudaError_t conv_tc(const ConvArgs &a, int, unsigned *err, cudaStream_t st) {
-    if (a.cin % 16 || a.cout % 16 || a.ldx % 16 || a.xoff % 16 || a.xoff + a.cin > a.ldx ||
-        (a.y && (a.ldy % 16 || a.yoff % 16 || a.yoff + a.cout > a.ldy)) ||
-        (a.yf && (a.ldyf % 16 || a.yfoff % 16 || a.yfoff + a.cout > a.ldyf)) ||
-        (a.ks != 1 && a.ks != 3) || a.B < 1 || a.H < 1 || a.W < 1 || (a.up2 && !a.y))
-        return cudaErrorInvalidValue;
+    if (!conv_args_ok(a)) return cudaErrorInvalidValue;
     if (a.cin % 64 == 0) return conv_tc_n<64>(a, err, st);
     if (a.cin % 32 == 0) return conv_tc_n<32>(a, err, st);
     return conv_tc_n<16>(a, err, st);
@@ -1078,15 +1084,15 @@ __global__ void __launch_bounds__(kTcThreads) k_wgrad_tc(const __grid_constant__
 }
 
 // Tensor map of a BF16 NHWC tensor's channel slice [0, C) (channel stride ld
-// elements) with boxes of {bc channels, 16, 8, 1}, swizzle span bc * 2 bytes.
+// elements) with boxes of {bc channels, bx, by, 1}, swizzle span bc * 2 bytes.
 cudaError_t encode_nhwc(CUtensorMap *tm, const bf16 *base, int C, int ld, int W, int H, int B,
-                        int bc, CUtensorMapL2promotion l2) {
+                        int bc, CUtensorMapL2promotion l2, int bx = kTileX, int by = kTileY) {
     const auto enc = tmap_encoder();
     if (!enc) return cudaErrorNotSupported;
     const cuuint64_t d[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
     const cuuint64_t s[3] = {(cuuint64_t)ld * 2, (cuuint64_t)ld * 2 * W,
                              (cuuint64_t)ld * 2 * W * H};
-    const cuuint32_t box[4] = {(cuuint32_t)bc, kTileX, kTileY, 1};
+    const cuuint32_t box[4] = {(cuuint32_t)bc, (cuuint32_t)bx, (cuuint32_t)by, 1};
     const cuuint32_t one[4] = {1, 1, 1, 1};
     const CUtensorMapSwizzle swz = bc == 64   ? CU_TENSOR_MAP_SWIZZLE_128B
                                    : bc == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
@@ -1151,6 +1157,248 @@ cudaError_t wgrad_tc(const WgArgs &a, unsigned *err, cudaStream_t st) {
     return wgrad_tc_n<16>(a, err, st);
 }
 
+// ---------------------------------------------------------------------------
+// Strip variant of the 3x3 convolution, for images whose width is a multiple
+// of 128 and at most 64 input and 64 output channels (CK = cin, NT = cout):
+// the tile is 128 consecutive pixels of one image row.  Per tile the TMA warp
+// loads the three halo strips {cin, 130, 1, 1} of rows y-1, y, y+1 (pixels
+// x0-1 .. x0+128, zeros outside the image) into one stage, and the MMA warp
+// issues the nine taps as MMAs on views of those strips that start 0, 1 or 2
+// rows in.  The swizzle is a function of the absolute shared-memory address,
+// so a view starting at any row of a strip written by TMA is a valid K-major
+// operand (descriptor base offset 0; checked on the hardware for the 128-
+// and 64-byte swizzles at every row shift 0 .. 7).  The nine taps' weights
+// stay resident in shared memory for the block's lifetime.  Per tile this
+// moves 3 x 130 TMA rows instead of 9 x (128 + NT); TMA issue (about one row
+// per three clocks per SM) bounds the patch variant on these layers.
+// ---------------------------------------------------------------------------
+constexpr int kStripW = 128, kStripRows = kStripW + 2;
+
+__host__ __device__ constexpr int strip_region(int ck) {  // one halo strip, 1024-aligned
+    return (kStripRows * ck * 2 + 1023) / 1024 * 1024;
+}
+__host__ __device__ constexpr int strip_wtap(int ck, int nt) {  // one tap's weights
+    return (nt * ck * 2 + 1023) / 1024 * 1024;
+}
+__host__ __device__ constexpr int strip_stages(int ck, int nt) {  // ~200 KB in all
+    return (200 * 1024 - 9 * strip_wtap(ck, nt)) / (3 * strip_region(ck)) < 2
+               ? 2
+               : ((200 * 1024 - 9 * strip_wtap(ck, nt)) / (3 * strip_region(ck)) > 6
+                      ? 6
+                      : (200 * 1024 - 9 * strip_wtap(ck, nt)) / (3 * strip_region(ck)));
+}
+__host__ __device__ constexpr int strip_smem(int ck, int nt) {
+    return 9 * strip_wtap(ck, nt) + strip_stages(ck, nt) * 3 * strip_region(ck) + 1024;
+}
+
+template <int CK, int NT>
+__global__ void __launch_bounds__(kTcThreads) k_conv_strip(const __grid_constant__ CUtensorMap tmx,
+                                                            const __grid_constant__ CUtensorMap tmw,
+                                                            ConvArgs a, int strips_x,
+                                                            unsigned *err) {
+    constexpr int REG = strip_region(CK);
+    constexpr int STAGE = 3 * REG;
+    constexpr int WTAP = strip_wtap(CK, NT);
+    constexpr int S = strip_stages(CK, NT);
+    constexpr int ACOLS = NT < 32 ? 32 : NT;
+    constexpr int TCOLS = 2 * ACOLS;
+    constexpr uint32_t IDESC = umma_idesc_bf16(kTcM, NT);
+    constexpr unsigned LAYOUT = sw_layout(CK);
+    constexpr unsigned SBO = 8 * CK * 2;
+    constexpr unsigned ROWB = CK * 2;  // bytes of one pixel row of a strip
+    extern __shared__ unsigned char smraw[];
+    __shared__ __align__(8) uint64_t full[S], empty[S], acc_full[2], acc_empty[2], wbar;
+    __shared__ uint32_t tmem_sh;
+    unsigned char *sm = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
+    unsigned char *sw = sm;                 // weights [tap][WTAP]
+    unsigned char *sst = sm + 9 * WTAP;     // stages [S][dy][REG]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n_tiles = strips_x * a.H * a.B;
+    auto tile_of = [&](int t) {
+        TcTile T;
+        T.x0 = (t % strips_x) * kStripW;
+        t /= strips_x;
+        T.y0 = t % a.H;
+        T.b = t / a.H;
+        T.n0 = 0;
+        return T;
+    };
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_sh)),
+                     "r"(TCOLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&acc_full[i], 1);
+            mbar_init(&acc_empty[i], 4);
+        }
+        mbar_init(&wbar, 1);
+        fence_mbar_init();
+    }
+    if (warp == 4 && lane == 0) {
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmx)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmw)) : "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = tmem_sh;
+
+    if (warp == 4) {
+        if (lane == 0) {  // TMA producer: the weights once, then three strips per tile
+            bool ok = true;
+            mbar_arrive_expect_tx(&wbar, 9u * NT * CK * 2);
+            for (int tap = 0; tap < 9; ++tap)
+                tma_load_2d(sw + tap * WTAP, &tmw, tap * a.cin, 0, &wbar);
+            int g = 0;
+            for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++g) {
+                const TcTile T = tile_of(t);
+                const int s = g % S;
+                const unsigned u = (unsigned)(g / S);
+                if (g >= S && !mbar_wait_tc(&empty[s], (u - 1) & 1)) ok = false;
+                unsigned char *st = sst + s * STAGE;
+                mbar_arrive_expect_tx(&full[s], 3u * kStripRows * CK * 2);
+                for (int d = 0; d < 3; ++d)
+                    tma_load_4d(st + d * REG, &tmx, 0, T.x0 - 1, T.y0 + d - 1, T.b, &full[s]);
+            }
+            if (!ok && err) atomicOr(err, DEV_ERR_TIMEOUT);
+        }
+        __syncwarp();
+    } else if (warp == 5) {
+        if (lane == 0) {  // MMA issuer: nine taps per tile
+            bool ok = mbar_wait_tc(&wbar, 0);
+            int it = 0;
+            for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+                const int ab = it & 1;
+                const unsigned au = (unsigned)(it >> 1);
+                if (it >= 2 && !mbar_wait_tc(&acc_empty[ab], (au - 1) & 1)) ok = false;
+                const int s = it % S;
+                if (!mbar_wait_tc(&full[s], (unsigned)(it / S) & 1)) ok = false;
+                tc_fence_after();
+                const uint32_t dacc = tmem + (uint32_t)(ab * ACOLS);
+                const unsigned st = smem_u32(sst + s * STAGE);
+                const unsigned sb = smem_u32(sw);
+#pragma unroll
+                for (int tap = 0; tap < 9; ++tap) {
+                    // output pixel i reads strip (tap / 3) at row i + tap % 3
+                    const unsigned av = st + (tap / 3) * REG + (tap % 3) * ROWB;
+                    const unsigned bv = sb + tap * WTAP;
+#pragma unroll
+                    for (int kk = 0; kk < CK / 16; ++kk) {
+                        const uint64_t da = umma_desc_sw(av + kk * 32, SBO, LAYOUT);
+                        const uint64_t db = umma_desc_sw(bv + kk * 32, SBO, LAYOUT);
+                        const uint32_t acc = (tap > 0 || kk > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
+                                dacc),
+                            "l"(da), "l"(db), "r"(IDESC), "r"(acc)
+                            : "memory");
+                    }
+                }
+                asm volatile(
+                    "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 "
+                    "[%0];" ::"r"(smem_u32(&empty[s]))
+                    : "memory");
+                asm volatile(
+                    "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 "
+                    "[%0];" ::"r"(smem_u32(&acc_full[ab]))
+                    : "memory");
+            }
+            if (!ok && err) atomicOr(err, DEV_ERR_TIMEOUT);
+        }
+        __syncwarp();
+    } else {  // epilogue
+        int it = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+            const TcTile T = tile_of(t);
+            const int ab = it & 1;
+            const unsigned au = (unsigned)(it >> 1);
+            if (!mbar_wait_tc(&acc_full[ab], au & 1)) {
+                if (err && lane == 0) atomicOr(err, DEV_ERR_TIMEOUT);
+                mbar_wait_tc(&acc_full[ab], au & 1);  // once more, bounded
+            }
+            tc_fence_after();
+            conv_tc_store<NT, true>(
+                a, T, tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(ab * ACOLS),
+                warp * 32 + lane);
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive_local(&acc_empty[ab]);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 5)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TCOLS)
+                     : "memory");
+}
+
+template <int CK, int NT>
+cudaError_t launch_conv_strip(const ConvArgs &a, unsigned *err, cudaStream_t st) {
+    constexpr int SMEM = strip_smem(CK, NT);
+    static_assert(SMEM <= 227 * 1024, "strip stages exceed shared memory");
+    U_TRY(cudaFuncSetAttribute(k_conv_strip<CK, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               SMEM));
+    CUtensorMap tmx, tmw;
+    U_TRY(encode_nhwc(&tmx, a.x + a.xoff, a.cin, a.ldx, a.W, a.H, a.B, CK,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, kStripRows, 1));
+    const auto enc = tmap_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    const int K = 9 * a.cin;
+    const cuuint64_t wd[2] = {(cuuint64_t)K, (cuuint64_t)a.cout};
+    const cuuint64_t ws[1] = {(cuuint64_t)K * 2};
+    const cuuint32_t wb[2] = {(cuuint32_t)CK, (cuuint32_t)NT};
+    const cuuint32_t one[2] = {1, 1};
+    const CUtensorMapSwizzle swz = CK == 64   ? CU_TENSOR_MAP_SWIZZLE_128B
+                                   : CK == 32 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                              : CU_TENSOR_MAP_SWIZZLE_32B;
+    if (enc(&tmw, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)a.w, wd, ws, wb, one,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
+    int dev = 0, sms = 148, per_sm = 1;
+    U_TRY(cudaGetDevice(&dev));
+    U_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    U_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv_strip<CK, NT>,
+                                                        kTcThreads, SMEM));
+    const int strips_x = a.W / kStripW;
+    const long long n_tiles = (long long)strips_x * a.H * a.B;
+    if (n_tiles > 0x7fffffffLL) return cudaErrorInvalidValue;
+    const int grid = (int)std::min<long long>(n_tiles, (long long)sms * std::max(per_sm, 1));
+    k_conv_strip<CK, NT><<<grid, kTcThreads, SMEM, st>>>(tmx, tmw, a, strips_x, err);
+    return cudaGetLastError();
+}
+
+template <int CK>
+cudaError_t conv_strip_n(const ConvArgs &a, unsigned *err, cudaStream_t st) {
+    if (a.cout == 16) return launch_conv_strip<CK, 16>(a, err, st);
+    if (a.cout == 32) return launch_conv_strip<CK, 32>(a, err, st);
+    return launch_conv_strip<CK, 64>(a, err, st);
+}
+
+bool conv_strip_fits(const ConvArgs &a) {
+    return a.ks == 3 && !a.up2 && a.W % kStripW == 0 &&
+           (a.cin == 16 || a.cin == 32 || a.cin == 64) &&
+           (a.cout == 16 || a.cout == 32 || a.cout == 64);
+}
+
+cudaError_t conv_strip(const ConvArgs &a, unsigned *err, cudaStream_t st) {
+    if (!conv_args_ok(a) || !conv_strip_fits(a)) return cudaErrorInvalidValue;
+    if (a.cin == 64) return conv_strip_n<64>(a, err, st);
+    if (a.cin == 32) return conv_strip_n<32>(a, err, st);
+    return conv_strip_n<16>(a, err, st);
+}
+
 int gridn_u(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 32); }
 
 constexpr int kLossBlocks = 296;
@@ -1188,6 +1436,8 @@ cudaError_t UNet::setup(int batch, int H, int W, unsigned long long seed, cudaSt
     err_ = err;
     const char *wm = std::getenv("IMP_UNET_WMMA");
     use_tc_ = !(wm && wm[0] == '1');
+    const char *ws = std::getenv("IMP_UNET_STRIP");
+    use_strip_ = !(ws && ws[0] == '0');
     B_ = batch;
     H_ = H;
     W_ = W;
@@ -1312,10 +1562,15 @@ cudaError_t UNet::conv_fwd(int li, const Act &in, int in_off, Act &out, int out_
     return run_conv(a, P);
 }
 
-// Tensor-memory (tcgen05) kernel unless IMP_UNET_WMMA=1 selects the WMMA one.
+// Tensor-memory (tcgen05) kernels unless IMP_UNET_WMMA=1 selects the WMMA
+// one: the strip variant where it applies (IMP_UNET_STRIP=0 turns it off),
+// else the 8 x 16 patch variant.
 cudaError_t UNet::run_conv(const ConvArgs &a, int P) {
     ++launches_;
-    if (use_tc_) return conv_tc(a, P, err_, st_);
+    if (use_tc_) {
+        if (use_strip_ && conv_strip_fits(a)) return conv_strip(a, err_, st_);
+        return conv_tc(a, P, err_, st_);
+    }
     const dim3 grid((P + 63) / 64, (a.cout + 63) / 64);
     if (a.cin % 32 == 0)
         k_conv_fwd<32><<<grid, kCT, 0, st_>>>(a);

@@ -92,6 +92,7 @@ private:
     long launches_ = 0;
     unsigned *err_ = nullptr;  // device error word (bounded-wait timeouts)
     bool use_tc_ = true;       // tcgen05 convolutions (else WMMA)
+    bool use_strip_ = true;    // row-strip variant for the layers it fits
 };
 
 }  // namespace imp

@@ -98,6 +98,34 @@ def test_training_reduces_loss(pkg, ctx):
     assert losses[-1] < 0.2 * losses[0]
 
 
+def test_row_strip_convolutions(pkg, ctx, monkeypatch):
+    """16 x 256 images: the 3x3 layers with <= 64 channels at widths 256 and 128
+    run the row-strip kernel (halo strips, taps as shifted shared-memory views).
+    Forward within 1e-2 of the BF16-emulating oracle; forward and gradients
+    equal to the 8 x 16 patch kernel's up to FP32 summation order."""
+    B, H, W = 1, 16, 256
+    x, t = data(B, H, W, 9)
+    res = {}
+    for name, env in (("strip", "1"), ("patch", "0")):
+        monkeypatch.setenv("IMP_UNET_STRIP", env)
+        net = pkg.UNet(ctx, B, H, W, seed=31)
+        try:
+            p = net.get_params()
+            y = net.forward(x, np.zeros_like(x))
+            loss, g = net.gradients(x, t)
+        finally:
+            net.close()
+        res[name] = (y, loss, g)
+    want, _ = U.forward(p, x, H, W, emulate_bf16=True)
+    e = rel(res["strip"][0], want.detach().numpy())
+    es, eg = rel(res["strip"][0], res["patch"][0]), rel(res["strip"][2], res["patch"][2])
+    print(f"strip vs oracle {e:.2e}; strip vs patch: forward {es:.2e}, gradients {eg:.2e}")
+    assert e < 1e-2
+    assert es < 1e-5
+    assert abs(res["strip"][1] - res["patch"][1]) / res["patch"][1] < 1e-4
+    assert eg < 1e-3
+
+
 def test_tensor_memory_and_wmma_kernels_agree(pkg, ctx, monkeypatch):
     """The tcgen05 convolution (accumulator in tensor memory) and the WMMA one
     give the same forward pass and gradients up to FP32 summation order."""
