@@ -82,6 +82,37 @@ def test_bf_3d_tv_matches_oracle(pkg, ctx, synth):
     assert oracle.rel_l2(x, ref) < TOL_IMG
 
 
+def test_batch_3d_tv_matches_oracle(pkg, ctx, synth):
+    """Batched multi-slice with the true 3-D phase and 3-D TV: two 24x24x8
+    slices with their own stacks of spirals, the second one shorter (uneven
+    M), each within 1e-4 of the FP64 oracle."""
+    cases = [small_3d(synth, seed=41), small_3d(synth, seed=42)]
+    keep = cases[1]["kx"].size - 640  # drop the last 640 samples of slice 1
+    c1 = cases[1]
+    C = np.asarray(c1["sens"]).size // c1["ix"].size
+    kd1 = np.asarray(c1["kdata"]).reshape(C, -1)[:, :keep]
+    cases[1] = dict(c1, kx=c1["kx"][:keep], ky=c1["ky"][:keep], kz=c1["kz"][:keep],
+                    t=c1["t"][:keep], kdata=kd1)
+    f32 = lambda a: np.ascontiguousarray(a, np.float32)
+    N = cases[0]["ix"].size
+    k_off = np.cumsum([0] + [c["kx"].size for c in cases])
+    cat = lambda k: f32(np.concatenate([np.ravel(c[k]) for c in cases]))
+    kd = np.concatenate([np.asarray(c["kdata"]).ravel() for c in cases])
+    sens = np.asarray(cases[0]["sens"]).reshape(C, N)
+    xr, xi = np.zeros(2 * N, np.float32), np.zeros(2 * N, np.float32)
+    opts = pkg.bf_options(cg_num=3, fd_penalizer=1e-2, tv=True, tv_num=2, use_z=1,
+                          dims=cases[0]["dims"])
+    pkg.bruteForceBatch(ctx, opts, xr, xi, f32(kd.real), f32(kd.imag), cat("kx"), cat("ky"),
+                        cat("kz"), cat("t"), k_off, cases[0]["ix"], cases[0]["iy"],
+                        cases[0]["iz"], cat("fm"), f32(sens.real), f32(sens.imag), N, C)
+    for s, c in enumerate(cases):
+        got = xr[s * N:(s + 1) * N] + 1j * xi[s * N:(s + 1) * N].astype(np.float64)
+        # the batch shares slice 0's coil maps; the oracle solves the same model
+        ref = oracle.bf_cg(dict(c, sens=cases[0]["sens"]), cg_num=3, lam=1e-2, tv=True,
+                           tv_num=2, eps=1e-6, use_z=1)
+        assert oracle.rel_l2(got, ref) < TOL_IMG, s
+
+
 def test_host_and_device_pointers_agree(pkg, ctx):
     from gpu_util import gpu_recon
     c = golden("bf_2d_c3")
