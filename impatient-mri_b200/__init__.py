@@ -38,6 +38,7 @@ EXPORTED = [
     "imp_abi_version", "imp_status_string", "imp_last_error",
     "imp_context_create", "imp_context_destroy", "imp_context_synchronize",
     "imp_context_launch_count", "imp_context_profile", "imp_context_profile_read",
+    "imp_check_wait_expiry",
     "imp_ft", "imp_ift", "imp_parallel_ft", "imp_parallel_ift", "imp_parallel_ift_noalloc",
     "imp_bf_options_default", "imp_bruteforce_recon", "imp_bruteforce_dir",
     "imp_bruteforce_batch", "imp_bruteforce_mgpu",
@@ -92,6 +93,7 @@ def lib() -> ctypes.CDLL:
         L.imp_context_destroy.argtypes = [vp]
         L.imp_context_synchronize.argtypes = [vp]
         L.imp_context_launch_count.argtypes = [vp]
+        L.imp_check_wait_expiry.argtypes = [vp, ip]
         L.imp_context_launch_count.restype = ctypes.c_long
         L.imp_context_profile.argtypes = [vp, ip]
         L.imp_context_profile_read.argtypes = [vp, ip, ctypes.POINTER(ctypes.c_double),
@@ -157,6 +159,11 @@ class Context:
 
     def launch_count(self) -> int:
         return int(lib().imp_context_launch_count(self._h))
+
+    def check_wait_expiry(self, polls: int = 1000) -> None:
+        """Runs a kernel whose bounded wait runs out; raises ImpError
+        (IMP_ERR_TIMEOUT) as every expired wait does."""
+        _check(lib().imp_check_wait_expiry(self._h, polls))
 
     def synchronize(self) -> None:
         _check(lib().imp_context_synchronize(self._h))

@@ -61,6 +61,24 @@ imp_status finish(imp_context *ctx) {
     return IMP_OK;
 }
 
+namespace {
+// One block whose bounded wait on an mbarrier that nothing ever arrives on
+// runs out after `polls` rounds: it records DEV_ERR_TIMEOUT and returns.
+__global__ void k_wait_expiry(unsigned *err, unsigned polls) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        bool done = false;
+        for (unsigned it = 0; it < polls && !done; ++it) done = mbar_try_wait(&bar, 0);
+        if (!done) atomicOr(err, DEV_ERR_TIMEOUT);
+    }
+}
+}  // namespace
+
 }  // namespace imp
 
 using imp::begin;
@@ -553,6 +571,16 @@ imp_status imp_bruteforce_batch(imp_context *ctx, const imp_bf_options *opt, flo
     s = finish(ctx);
     ctx->launches = launches;
     return s;
+}
+
+imp_status imp_check_wait_expiry(imp_context *ctx, int polls) {
+    if (!ctx || polls <= 0) return fail(IMP_ERR_INVALID_ARG, "null context or polls <= 0");
+    imp_status s = begin(ctx);
+    if (s != IMP_OK) return s;
+    imp::k_wait_expiry<<<1, 32, 0, ctx->stream>>>(ctx->dev_err, (unsigned)polls);
+    IMP_CUDA(cudaGetLastError(), "wait-expiry kernel");
+    ctx->launches = 1;
+    return finish(ctx);  // IMP_ERR_TIMEOUT, read from the device error word
 }
 
 imp_status imp_context_profile(imp_context *ctx, int enable) {

@@ -59,6 +59,13 @@ imp_status imp_context_profile(imp_context *ctx, int enable);
 imp_status imp_context_profile_read(const imp_context *ctx, int which, double *total_ms,
                                     long *count);
 
+/* Runs one kernel whose bounded mbarrier wait runs out (a barrier nothing
+ * arrives on, `polls` try_wait rounds): the failure path of every bounded
+ * wait in the library's kernels.  Returns IMP_ERR_TIMEOUT with its message;
+ * the kernel ends normally and the context stays usable.  No reference
+ * counterpart (the reference's kernels have no device-side waits). */
+imp_status imp_check_wait_expiry(imp_context *ctx, int polls);
+
 /* Measures the FP32 FMA rate (TFLOP/s, 2 flops per FMA) and the SFU sine rate
  * (G ops/s) of `device` with two short throughput kernels: the denominators
  * of the NUDFT roofline.  No reference counterpart. */

@@ -113,6 +113,22 @@ def test_batch_3d_tv_matches_oracle(pkg, ctx, synth):
         assert oracle.rel_l2(got, ref) < TOL_IMG, s
 
 
+def test_expired_wait_is_reported_and_context_stays_usable(pkg):
+    """Failure path of the bounded device-side waits, without a GPU fault: a
+    kernel waits on an mbarrier nothing arrives on, gives up after 1000 rounds,
+    records the timeout and returns; the call reports IMP_ERR_TIMEOUT and the
+    same context then reconstructs within 1e-4 of the FP64 oracle."""
+    from gpu_util import gpu_recon
+    with pkg.Context(0) as c0:
+        with pytest.raises(pkg.ImpError) as e:
+            c0.check_wait_expiry(1000)
+        assert e.value.status == 7 and "wait" in str(e.value)
+        c = golden("bf_2d_c3")
+        x = gpu_recon(pkg, c0, c, cg_num=3, lam=1e-2, tv=False)
+    ref = oracle.bf_cg(c, cg_num=3, lam=1e-2, tv=False, eps=1e-6, use_z=0)
+    assert oracle.rel_l2(x, ref) < TOL_IMG
+
+
 def test_host_and_device_pointers_agree(pkg, ctx):
     from gpu_util import gpu_recon
     c = golden("bf_2d_c3")
