@@ -15,6 +15,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <vector>
 
@@ -210,6 +211,20 @@ struct PlaneGeo {
     int lnm, lnf, lplane, lr2m, lr2f, lps;  // log2 of nm, nf, nm*nf, r2m, r2f, ps
 };
 
+// The same geometry with the plane sizes as compile-time constants (the slow
+// size and the coil count stay runtime): the plane kernels instantiated on it
+// fold their per-element index arithmetic into immediates.
+template <int NM, int NF, int PS>
+struct PlaneGeoC {
+    static constexpr int nm = NM, nf = NF, ps = PS, qm = NM > 1 ? 2 : 1, rs = NF + 1;
+    static constexpr int ncol = qm * 2 * NM * NF;
+    static constexpr int r1m = split_r1(NM), r2m = NM / r1m;
+    static constexpr int r1f = split_r1(NF), r2f = NF / r1f;
+    static constexpr int lnm = ilog2c(NM), lnf = ilog2c(NF), lplane = lnm + lnf;
+    static constexpr int lr2m = ilog2c(r2m), lr2f = ilog2c(r2f), lps = ilog2c(PS);
+    int ns, C;
+};
+
 // Bounded mbarrier wait (about 2^22 polls); false when it ran out.
 __device__ __forceinline__ bool wait_bounded(uint64_t *bar, unsigned parity) {
     for (unsigned it = 0; it < (1u << 22); ++it)
@@ -222,10 +237,10 @@ __device__ __forceinline__ bool wait_bounded(uint64_t *bar, unsigned parity) {
 // shared memory (U); each (am, af) parity quadrant is then twiddled into the
 // work plane P, transformed, and written to b1[c][s][am][af][km][kf] in
 // natural frequency order.
-template <int VPT>
+template <int VPT, class Geo = PlaneGeo>
 __global__ void __launch_bounds__(kPlaneThreads) k_fwd_plane(
     float2 *__restrict__ b1, const float2 *__restrict__ x, const float2 *__restrict__ sens,
-    const float2 *__restrict__ eph_l, PlaneGeo g, const float2 *__restrict__ tw,
+    const float2 *__restrict__ eph_l, Geo g, const float2 *__restrict__ tw,
     const int *__restrict__ done) {
     extern __shared__ float2 smem[];
     if (done && *done) return;
@@ -303,10 +318,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fwd_plane(
 // 1/csize share of the plane), applies conj(e_l) and writes (first) or
 // accumulates q.  A copy that does not complete within the bounded wait sets
 // DEV_ERR_TIMEOUT in *err and ends the block's work early.
-template <int VPT>
+template <int VPT, class Geo = PlaneGeo>
 __global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
     float2 *__restrict__ q, const float2 *__restrict__ b1, const float2 *__restrict__ sens,
-    const float2 *__restrict__ eph_l, PlaneGeo g, int first, const float2 *__restrict__ tw,
+    const float2 *__restrict__ eph_l, Geo g, int first, const float2 *__restrict__ tw,
     const int *__restrict__ done, unsigned *err) {
     extern __shared__ __align__(16) float2 smem[];
     __shared__ __align__(8) uint64_t bar;
@@ -524,13 +539,34 @@ __global__ void k_qf_perm(float2 *__restrict__ qf2, const float2 *__restrict__ q
 
 bool pow2(int n) { return n >= 1 && (n & (n - 1)) == 0; }
 
-template <int VPT>
+template <int VPT, class Geo = PlaneGeo>
 cudaError_t set_plane_smem(size_t fwd_bytes, size_t inv_bytes) {
     cudaError_t e = cudaFuncSetAttribute(
-        k_fwd_plane<VPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_bytes);
+        k_fwd_plane<VPT, Geo>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_bytes);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_inv_plane<VPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)inv_bytes);
+    return cudaFuncSetAttribute(k_inv_plane<VPT, Geo>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_bytes);
+}
+
+// Plane geometries with compile-time instantiations: 3-D 256 x 256 x 32 images
+// (planes of 256 x 32, one per block) and 2-D 512 x 512 images (rows of 512,
+// 16 per block).  Others run the generic (runtime-geometry) kernels.
+using GeoC3d = PlaneGeoC<256, 32, 1>;
+using GeoC2d = PlaneGeoC<1, 512, 16>;
+// IMP_TOEP_GENERIC=1 keeps the generic kernels (the tests compare both).
+int spec_kind(const ToepFftPlan &p) {
+    const char *gen = std::getenv("IMP_TOEP_GENERIC");
+    if (gen && gen[0] == '1') return 0;
+    if (p.vpt == 16 && p.nm == 256 && p.nf == 32 && p.ps == 1) return 1;
+    if (p.vpt == 16 && p.nm == 1 && p.nf == 512 && p.ps == 16) return 2;
+    return 0;
+}
+template <class G>
+G geo_c(const ToepFftPlan &p) {
+    G g;
+    g.ns = p.ns;
+    g.C = p.C;
+    return g;
 }
 
 template <int NS>
@@ -603,6 +639,10 @@ bool toep_fft_plan(int ns, int nm, int nf, int C, ToepFftPlan *plan) {
         default: return false;
     }
     if (e != cudaSuccess) return false;
+    p.spec = spec_kind(p);
+    if (p.spec == 1) e = set_plane_smem<16, GeoC3d>(p.smem_plane, p.smem_inv);
+    if (p.spec == 2) e = set_plane_smem<16, GeoC2d>(p.smem_plane, p.smem_inv);
+    if (e != cudaSuccess) return false;
     switch (ns) {
         case 2: e = set_slow_smem<2>(p.smem_slow); break;
         case 4: e = set_slow_smem<4>(p.smem_slow); break;
@@ -645,19 +685,28 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
                              unsigned *err, cudaStream_t st) {
     const PlaneGeo g = geo_of(p);
     const dim3 ga(p.ns / p.ps, p.C);
+    const int spec = p.spec;
 #define IMP_PLANE_CASE(V)                                                                   \
     case V:                                                                                 \
         k_fwd_plane<V><<<ga, kPlaneThreads, p.smem_plane, st>>>(b1, x, sens, eph_l, g, tw,  \
                                                                 done);                      \
         break;
-    switch (p.vpt) {
-        IMP_PLANE_CASE(1)
-        IMP_PLANE_CASE(2)
-        IMP_PLANE_CASE(4)
-        IMP_PLANE_CASE(8)
-        IMP_PLANE_CASE(16)
-        IMP_PLANE_CASE(32)
-        default: return cudaErrorInvalidValue;
+    if (spec == 1) {
+        k_fwd_plane<16, GeoC3d><<<ga, kPlaneThreads, p.smem_plane, st>>>(
+            b1, x, sens, eph_l, geo_c<GeoC3d>(p), tw, done);
+    } else if (spec == 2) {
+        k_fwd_plane<16, GeoC2d><<<ga, kPlaneThreads, p.smem_plane, st>>>(
+            b1, x, sens, eph_l, geo_c<GeoC2d>(p), tw, done);
+    } else {
+        switch (p.vpt) {
+            IMP_PLANE_CASE(1)
+            IMP_PLANE_CASE(2)
+            IMP_PLANE_CASE(4)
+            IMP_PLANE_CASE(8)
+            IMP_PLANE_CASE(16)
+            IMP_PLANE_CASE(32)
+            default: return cudaErrorInvalidValue;
+        }
     }
 #undef IMP_PLANE_CASE
     const int r1 = split_r1(p.ns);
@@ -696,7 +745,13 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cudaError_t e;
-    switch (p.vpt) {
+    if (spec == 1)
+        e = cudaLaunchKernelEx(&cfg, k_inv_plane<16, GeoC3d>, q, b1, sens, eph_l,
+                               geo_c<GeoC3d>(p), first, tw, done, err);
+    else if (spec == 2)
+        e = cudaLaunchKernelEx(&cfg, k_inv_plane<16, GeoC2d>, q, b1, sens, eph_l,
+                               geo_c<GeoC2d>(p), first, tw, done, err);
+    else switch (p.vpt) {
         case 1: e = cudaLaunchKernelEx(&cfg, k_inv_plane<1>, q, b1, sens, eph_l, g, first, tw, done, err); break;
         case 2: e = cudaLaunchKernelEx(&cfg, k_inv_plane<2>, q, b1, sens, eph_l, g, first, tw, done, err); break;
         case 4: e = cudaLaunchKernelEx(&cfg, k_inv_plane<4>, q, b1, sens, eph_l, g, first, tw, done, err); break;

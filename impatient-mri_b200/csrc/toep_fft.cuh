@@ -33,6 +33,7 @@ struct ToepFftPlan {
     int ncol = 0;                // spectrum columns per s: qm * 2 * nm * nf
     int W = 1;                   // columns per k_slow block
     int csize = 1;               // k_inv_plane cluster width (coil split), divides C, <= 8
+    int spec = 0;                // plane kernels with compile-time geometry (0 = generic)
     size_t smem_plane = 0, smem_inv = 0, smem_slow = 0;
     size_t b1_elems() const { return (size_t)C * ns * ncol; }
 };

@@ -191,6 +191,34 @@ def test_apply_sizes_match_oracle(pkg, ctx, dims, C, L):
     assert err < TOL_OP
 
 
+@pytest.mark.parametrize("dims", [(256, 256, 32), (512, 512, 1)])
+def test_specialised_plane_kernels_match_generic(pkg, monkeypatch, dims):
+    """The plane kernels instantiated on compile-time geometry (3-D 256x256x32
+    and 2-D 512x512 images) give the A^H A application of the generic
+    runtime-geometry kernels (which the oracle tests above cover)."""
+    rng = np.random.default_rng(sum(dims))
+    nx, ny, nz = dims
+    C, L, M = 2, 1, 64
+    N, G = nx * ny * nz, grid_elems(dims)
+    c = dict(dims=dims, L=L, cg=1, fdp=1e-2, tv_num=0, os_q=2.0, os_fh=1.5,
+             t=np.sort(rng.uniform(0.0, 0.01, M)).astype(np.float32),
+             kx=np.zeros(M, np.float32),
+             fm=rng.uniform(-300.0, 300.0, N).astype(np.float32),
+             sens=(rng.standard_normal((C, N)) + 1j * rng.standard_normal((C, N))).astype(
+                 np.complex64))
+    Q = (rng.standard_normal((L + 1, G)) + 1j * rng.standard_normal((L + 1, G))).astype(
+        np.complex64)
+    p = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    out = {}
+    for name, env in (("specialised", "0"), ("generic", "1")):
+        monkeypatch.setenv("IMP_TOEP_GENERIC", env)
+        with pkg.Context(0) as c0:  # the choice is made when the context plans
+            out[name] = gpu_apply(pkg, c0, opts_of(pkg, c), c, Q, p)
+    err = rel(out["specialised"], out["generic"])
+    print(f"apply {dims}: specialised vs generic {err:.2e}")
+    assert err < 1e-6
+
+
 def test_device_and_host_pointers_agree(pkg, ctx):
     c = load("toep_2d_tv")
     o = opts_of(pkg, c)
