@@ -441,17 +441,21 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
 // and written back in place.  blockDim = W * R1: thread (w, j1).
 constexpr int kSlowThreads = 256;
 
-template <int NS>
+// WC, NCOLC > 0: the block's column count W and the spectrum's column count
+// ncol as compile-time constants (the runtime arguments are then ignored).
+template <int NS, int WC = 0, int NCOLC = 0>
 __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
-    float2 *__restrict__ b1, const float2 *__restrict__ qf2, int C, int ncol, int W,
+    float2 *__restrict__ b1, const float2 *__restrict__ qf2, int C, int ncol_rt, int W_rt,
     const float2 *__restrict__ tw, const int *__restrict__ done) {
     constexpr int R1 = split_r1(NS), R2 = NS / R1;
     constexpr int LNS = ilog2c(NS);
+    const int W = WC > 0 ? WC : W_rt;
+    const int ncol = NCOLC > 0 ? NCOLC : ncol_rt;
     extern __shared__ float2 E[];       // [NS][W] work
     float2 *Y = E + NS * W;             // [NS][W] parity sum (each thread owns its slots)
     if (done && *done) return;
     const int col0 = blockIdx.x * W;
-    const int lw = __ffs(W) - 1;
+    const int lw = WC > 0 ? ilog2c(WC) : __ffs(W) - 1;
     const int w = threadIdx.x & (W - 1), j1 = threadIdx.x >> lw;
     const size_t per_coil = (size_t)NS * ncol;
     for (int c = blockIdx.y; c < C; c += gridDim.y) {  // coils split over blockIdx.y
@@ -569,10 +573,19 @@ G geo_c(const ToepFftPlan &p) {
     return g;
 }
 
-template <int NS>
+template <int NS, int WC = 0, int NCOLC = 0>
 cudaError_t set_slow_smem(size_t bytes) {
-    return cudaFuncSetAttribute(k_slow<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)bytes);
+    return cudaFuncSetAttribute(k_slow<NS, WC, NCOLC>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// Slow-axis instantiations with compile-time block and spectrum widths for the
+// two specialised geometries (only when the plan's W and ncol are the ones
+// compiled in).
+int slow_spec(const ToepFftPlan &p) {
+    if (p.spec == 1 && p.ns == 256 && p.W == 16 && p.ncol == 32768) return 1;
+    if (p.spec == 2 && p.ns == 512 && p.W == 8 && p.ncol == 1024) return 2;
+    return 0;
 }
 
 PlaneGeo geo_of(const ToepFftPlan &p) {
@@ -656,6 +669,9 @@ bool toep_fft_plan(int ns, int nm, int nf, int C, ToepFftPlan *plan) {
         default: e = set_slow_smem<1024>(p.smem_slow); break;
     }
     if (e != cudaSuccess) return false;
+    if (slow_spec(p) == 1) e = set_slow_smem<256, 16, 32768>(p.smem_slow);
+    if (slow_spec(p) == 2) e = set_slow_smem<512, 8, 1024>(p.smem_slow);
+    if (e != cudaSuccess) return false;
     *plan = p;
     return true;
 }
@@ -718,7 +734,14 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
         k_slow<NSV><<<blocks, threads, p.smem_slow, st>>>(b1, qf2_l, p.C, p.ncol, p.W, tw, \
                                                           done);                           \
         break;
-    switch (p.ns) {
+    const int sspec = slow_spec(p);
+    if (sspec == 1)
+        k_slow<256, 16, 32768><<<blocks, threads, p.smem_slow, st>>>(b1, qf2_l, p.C, p.ncol, p.W,
+                                                                   tw, done);
+    else if (sspec == 2)
+        k_slow<512, 8, 1024><<<blocks, threads, p.smem_slow, st>>>(b1, qf2_l, p.C, p.ncol, p.W,
+                                                                 tw, done);
+    else switch (p.ns) {
         IMP_SLOW_CASE(2)
         IMP_SLOW_CASE(4)
         IMP_SLOW_CASE(8)
