@@ -15,6 +15,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cstdlib>
 #include <cmath>
 #include <vector>
@@ -49,7 +50,7 @@ __device__ __forceinline__ int slot_of(int k, int r1, int lr2) {
 
 // w_n^e (conjugated when inv), n = 2^lg <= kTwN.
 __device__ __forceinline__ float2 wn(const float2 *__restrict__ tw, int e, int lg, bool inv) {
-    float2 w = __ldg(&tw[(e & ((1 << lg) - 1)) << (kTwLg - lg)]);
+    float2 w = tw[(e & ((1 << lg) - 1)) << (kTwLg - lg)];  // global or shared table
     if (inv) w.y = -w.y;
     return w;
 }
@@ -225,6 +226,13 @@ struct PlaneGeoC {
     int ns, C;
 };
 
+// The compile-time-geometry instantiations keep the twiddle table in shared
+// memory (kTwN float2 after their regions); the generic ones read it through
+// the read-only global path.
+template <class Geo>
+constexpr bool kSmemTw = !std::is_same<Geo, PlaneGeo>::value;
+constexpr size_t kTwBytes = kTwN * sizeof(float2);
+
 // Bounded mbarrier wait (about 2^22 polls); false when it ran out.
 __device__ __forceinline__ bool wait_bounded(uint64_t *bar, unsigned parity) {
     for (unsigned it = 0; it < (1u << 22); ++it)
@@ -240,10 +248,16 @@ __device__ __forceinline__ bool wait_bounded(uint64_t *bar, unsigned parity) {
 template <int VPT, class Geo = PlaneGeo>
 __global__ void __launch_bounds__(kPlaneThreads) k_fwd_plane(
     float2 *__restrict__ b1, const float2 *__restrict__ x, const float2 *__restrict__ sens,
-    const float2 *__restrict__ eph_l, Geo g, const float2 *__restrict__ tw,
+    const float2 *__restrict__ eph_l, Geo g, const float2 *__restrict__ tw_g,
     const int *__restrict__ done) {
     extern __shared__ float2 smem[];
     if (done && *done) return;
+    const float2 *tw = tw_g;
+    if constexpr (kSmemTw<Geo>) {  // twiddle table after the plane regions
+        float2 *tws = smem + (size_t)g.ps * g.nm * g.rs + ((size_t)g.ps << g.lplane);
+        for (int i = threadIdx.x; i < kTwN; i += kPlaneThreads) tws[i] = __ldg(&tw_g[i]);
+        tw = tws;  // first read after the __syncthreads opening the quadrant loop
+    }
     const int plane = 1 << g.lplane;
     const int s0 = blockIdx.x * g.ps, c = blockIdx.y;
     const int ecta = g.ps << g.lplane;
@@ -321,7 +335,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fwd_plane(
 template <int VPT, class Geo = PlaneGeo>
 __global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
     float2 *__restrict__ q, const float2 *__restrict__ b1, const float2 *__restrict__ sens,
-    const float2 *__restrict__ eph_l, Geo g, int first, const float2 *__restrict__ tw,
+    const float2 *__restrict__ eph_l, Geo g, int first, const float2 *__restrict__ tw_g,
     const int *__restrict__ done, unsigned *err) {
     extern __shared__ __align__(16) float2 smem[];
     __shared__ __align__(8) uint64_t bar;
@@ -335,6 +349,15 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
     const bool skip = done && *done;
     const int rank = blockIdx.y, csize = gridDim.y;
     const int s0 = blockIdx.x * g.ps;
+    const float2 *tw = tw_g;
+    if constexpr (kSmemTw<Geo>) {  // twiddle table after the three regions
+        if (!skip) {
+            float2 *tws = smem + 2 * (size_t)ecta + (size_t)g.ps * pstride;
+            for (int i = threadIdx.x; i < kTwN; i += kPlaneThreads) tws[i] = __ldg(&tw_g[i]);
+            __syncthreads();
+            tw = tws;
+        }
+    }
     if (!skip) {
         const size_t N = (size_t)g.ns << g.lplane;
         const size_t vbase = (size_t)s0 << g.lplane;
@@ -653,8 +676,9 @@ bool toep_fft_plan(int ns, int nm, int nf, int C, ToepFftPlan *plan) {
     }
     if (e != cudaSuccess) return false;
     p.spec = spec_kind(p);
-    if (p.spec == 1) e = set_plane_smem<16, GeoC3d>(p.smem_plane, p.smem_inv);
-    if (p.spec == 2) e = set_plane_smem<16, GeoC2d>(p.smem_plane, p.smem_inv);
+    if (p.smem_inv + kTwBytes > kMaxSmem) p.spec = 0;  // no room for the twiddle table
+    if (p.spec == 1) e = set_plane_smem<16, GeoC3d>(p.smem_plane + kTwBytes, p.smem_inv + kTwBytes);
+    if (p.spec == 2) e = set_plane_smem<16, GeoC2d>(p.smem_plane + kTwBytes, p.smem_inv + kTwBytes);
     if (e != cudaSuccess) return false;
     switch (ns) {
         case 2: e = set_slow_smem<2>(p.smem_slow); break;
@@ -708,10 +732,10 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
                                                                 done);                      \
         break;
     if (spec == 1) {
-        k_fwd_plane<16, GeoC3d><<<ga, kPlaneThreads, p.smem_plane, st>>>(
+        k_fwd_plane<16, GeoC3d><<<ga, kPlaneThreads, p.smem_plane + kTwBytes, st>>>(
             b1, x, sens, eph_l, geo_c<GeoC3d>(p), tw, done);
     } else if (spec == 2) {
-        k_fwd_plane<16, GeoC2d><<<ga, kPlaneThreads, p.smem_plane, st>>>(
+        k_fwd_plane<16, GeoC2d><<<ga, kPlaneThreads, p.smem_plane + kTwBytes, st>>>(
             b1, x, sens, eph_l, geo_c<GeoC2d>(p), tw, done);
     } else {
         switch (p.vpt) {
@@ -758,7 +782,7 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(p.ns / p.ps, p.csize);
     cfg.blockDim = dim3(kPlaneThreads);
-    cfg.dynamicSmemBytes = p.smem_inv;
+    cfg.dynamicSmemBytes = p.smem_inv + (spec ? kTwBytes : 0);
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
