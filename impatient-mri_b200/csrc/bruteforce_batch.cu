@@ -290,8 +290,10 @@ cudaError_t dalloc(T **p, size_t count) {
 
 // Split of the "theirs" range: about two waves of four blocks per SM, and
 // whole tiles for every slice's range (`ranges`).
-int batch_split(long long blocks, const std::vector<int> &ranges) {
-    const long long target = 148LL * 4 * 2;
+int batch_split(long long blocks, const std::vector<int> &ranges, bool tc) {
+    // two waves at four blocks per SM; the tensor-core kernel runs one block
+    // per SM and gets about eight waves
+    const long long target = tc ? 148LL * 8 : 148LL * 4 * 2;
     int split = 1;
     auto ok = [&](int sp) {
         for (int r : ranges)
@@ -381,9 +383,11 @@ cudaError_t BfBatch::setup(const BfConfig &cfg, int S, const int *k_off, const f
     // one launch shape for every slice
     fwd_ = nu_default_launch(plan_, false);
     adj_ = nu_default_launch(plan_, true);
-    fwd_.split = batch_split((long long)(mpad_total_ / (kNT * fwd_.pt)) * G,
-                             std::vector<int>{Npad});
-    adj_.split = batch_split((long long)(Npad / (kNT * adj_.pt)) * G * S, mpad_);
+    const int fwd_rows = fwd_.tc ? kTcRows : kNT * fwd_.pt;
+    const int adj_rows = adj_.tc ? kTcRows : kNT * adj_.pt;
+    fwd_.split = batch_split((long long)(mpad_total_ / fwd_rows) * G, std::vector<int>{Npad},
+                             fwd_.tc != 0);
+    adj_.split = batch_split((long long)(Npad / adj_rows) * G * S, mpad_, adj_.tc != 0);
     std::vector<NuSlice> tf(S), ta(S);
     std::vector<BbSlice> tv(S);
     for (int s = 0; s < S; ++s) {

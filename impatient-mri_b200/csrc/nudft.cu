@@ -18,6 +18,7 @@
 #include "common.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 
 namespace imp {
 
@@ -355,6 +356,9 @@ cudaError_t launch_nudft_batch(const NuPlan &p, const NuLaunch &l, int S, int ma
                                const NuSlice *sl, const double4 *ours, const double4 *theirs,
                                const float2 *tdata, float2 *out, unsigned *err,
                                cudaStream_t st) {
+    if (l.tc)
+        return nu_partials_tc_batch(p, l, ADJ, S, max_ours, sl, ours, theirs, tdata, out, err,
+                                    st);
 #define IMP_CASE(CGV, PTV)                                                                     \
     if (p.CG == CGV && l.pt == PTV) {                                                          \
         if (l.occ == 6)                                                                        \
@@ -376,6 +380,7 @@ cudaError_t launch_nudft_batch(const NuPlan &p, const NuLaunch &l, int S, int ma
 template <bool ADJ>
 cudaError_t launch_nudft(const NuPlan &p, const NuLaunch &l, const float2 *tdata, float2 *out,
                          unsigned *err, cudaStream_t st) {
+    if (l.tc) return nu_partials_tc(p, l, ADJ, tdata, out, err, st);
     const double4 *ours = ADJ ? p.vgeo : p.kgeo;
     const double4 *theirs = ADJ ? p.kgeo : p.vgeo;
 #define IMP_CASE(CGV, PTV)                                                                   \
@@ -402,6 +407,16 @@ bool nu_split_ok(int n_theirs, int split) {
            n_theirs / split >= kTile;
 }
 
+bool nu_tc_enabled() {
+    const char *e = std::getenv("IMP_NUDFT_TC");
+    return !(e && e[0] == '0');
+}
+
+bool nu_tc_forced() {
+    const char *e = std::getenv("IMP_NUDFT_TC");
+    return e && e[0] == '1';
+}
+
 bool nu_shape_supported(int CG, int pt) {
     return (CG == 1 && (pt == 4 || pt == 8)) || (CG == 2 && pt == 4) ||
            (CG == 4 && (pt == 2 || pt == 4)) || (CG == 8 && pt == 2);
@@ -421,6 +436,17 @@ NuLaunch nu_default_launch(const NuPlan &p, bool adj) {
     l.pt = p.CG >= 8 ? 2 : 4;
     const int n_ours = adj ? p.Npad : p.Mpad;
     const int n_theirs = adj ? p.Mpad : p.Npad;
+    if (nu_tc_forced() && nu_tc_supported(p.CG) && n_ours % kTcRows == 0) {
+        // one block per SM: about eight waves of blocks, whole tiles per split
+        l.tc = 1;
+        const long blocks = (long)(n_ours / kTcRows) * p.G;
+        int split = 1;
+        while (blocks * split < 148L * 8 && split < 64 && nu_split_ok(n_theirs, split * 2) &&
+               n_theirs / (split * 2) >= 4 * kTile)
+            split *= 2;
+        l.split = split;
+        return l;
+    }
     const long blocks = (long)(n_ours / (kNT * l.pt)) * p.G;
     const long target = 148L * 4 * 2;  // two waves at four blocks per SM
     int split = 1;

@@ -26,7 +26,10 @@ struct NuLaunch {
     int pt = 4;     // "ours" elements per thread
     int split = 1;  // partitions of the "theirs" range (partial sums)
     int occ = 4;    // blocks per SM the register budget is sized for (4 or 6)
+    int tc = 0;     // 1: tensor-core kernel (nudft_tc.cu; pt and occ unused)
 };
+
+constexpr int kTcRows = 256;  // "ours" rows per block of the tensor-core kernel
 
 struct NuPlan {
     int M = 0, N = 0, C = 0;     // samples, voxels, coils
@@ -118,7 +121,23 @@ bool nu_shape_supported(int CG, int pt);
 // True when `split` partitions n_theirs into whole shared-memory tiles.
 bool nu_split_ok(int n_theirs, int split);
 
+// Tensor-core kernel (nudft_tc.cu): same partial-sum layouts as
+// nu_forward_partials / nu_adjoint_partials / nu_partials_batch; coil groups
+// of 1, 2, 4 or 8.  It is an autotuner candidate unless IMP_NUDFT_TC=0
+// (nu_tc_enabled), and the default launch shape when IMP_NUDFT_TC=1
+// (nu_tc_forced).
+bool nu_tc_supported(int CG);
+bool nu_tc_enabled();
+bool nu_tc_forced();
+cudaError_t nu_partials_tc(const NuPlan &p, const NuLaunch &l, bool adj, const float2 *tdata,
+                           float2 *out, unsigned *dev_err, cudaStream_t st);
+cudaError_t nu_partials_tc_batch(const NuPlan &p, const NuLaunch &l, bool adj, int S,
+                                 int max_ours, const NuSlice *d_slices, const double4 *ours,
+                                 const double4 *theirs, const float2 *tdata, float2 *out,
+                                 unsigned *dev_err, cudaStream_t st);
+
 // Autotuner (tune.cu): times every supported (pt, occ, split) of one direction
+// and the tensor-core kernel's splits
 // on the live buffers `tdata` / `part` (part_bytes of scratch) and returns the
 // fastest.  Results are cached per problem shape in memory and in a text file
 // ($IMP_TUNE_CACHE, default ~/.cache/impatient_b200/nudft_tune.txt).

@@ -3,11 +3,13 @@
 // For one problem shape and direction it times every launch shape the kernel
 // set covers -- "ours" elements per thread (pt), register budget (occupancy
 // 4 or 6 blocks per SM) and the number of partitions of the "theirs" range
-// (split) -- with CUDA events on the launching stream, and keeps the fastest.
+// (split), and the tensor-core kernel at every split -- with CUDA events on
+// the launching stream, and keeps the fastest.
 // Results are cached per shape in memory and persisted as text lines
-//     v1 <adj> <CG> <G> <use_z> <Mpad> <Npad> <pt> <occ> <split> <ms>
+//     v2 <adj> <CG> <G> <use_z> <Mpad> <Npad> <pt> <occ> <split> <tc> <ms>
 // in $IMP_TUNE_CACHE (default ~/.cache/impatient_b200/nudft_tune.txt), so a
-// shape is tuned once per machine.  IMP_AUTOTUNE=0 turns tuning off.
+// shape is tuned once per machine.  IMP_AUTOTUNE=0 turns tuning and the use of
+// tuned shapes off (default launch shapes only).
 #include "nudft.cuh"
 
 #include <cstdio>
@@ -44,18 +46,21 @@ void load_locked() {
     g_loaded = true;
     FILE *f = std::fopen(cache_path().c_str(), "r");
     if (!f) return;
-    char tag[8];
-    int a, cg, g, z, mp, np, pt, occ, split;
-    double ms;
-    while (std::fscanf(f, "%7s %d %d %d %d %d %d %d %d %d %lf", tag, &a, &cg, &g, &z, &mp, &np,
-                       &pt, &occ, &split, &ms) == 11) {
-        if (std::string(tag) != "v1") continue;
+    char line[256];
+    while (std::fgets(line, sizeof line, f)) {
+        int a, cg, g, z, mp, np, pt, occ, split, tc;
+        double ms;
+        if (std::sscanf(line, "v2 %d %d %d %d %d %d %d %d %d %d %lf", &a, &cg, &g, &z, &mp, &np,
+                        &pt, &occ, &split, &tc, &ms) != 11)
+            continue;  // other versions are re-tuned
         NuLaunch l;
         l.pt = pt;
         l.occ = occ;
         l.split = split;
-        if (nu_shape_supported(cg, pt) && (occ == 4 || occ == 6))
-            g_cache[Key(a, cg, g, z, mp, np)] = l;
+        l.tc = tc;
+        const bool ok = tc ? (nu_tc_supported(cg) && nu_tc_enabled())
+                           : (nu_shape_supported(cg, pt) && (occ == 4 || occ == 6));
+        if (ok) g_cache[Key(a, cg, g, z, mp, np)] = l;
     }
     std::fclose(f);
 }
@@ -67,9 +72,9 @@ void persist(const Key &k, const NuLaunch &l, double ms) {
         if (path[i] == '/') mkdir(path.substr(0, i).c_str(), 0755);
     FILE *f = std::fopen(path.c_str(), "a");
     if (!f) return;  // the cache is an optimisation; failure to write is not an error
-    std::fprintf(f, "v1 %d %d %d %d %d %d %d %d %d %.4f\n", std::get<0>(k), std::get<1>(k),
+    std::fprintf(f, "v2 %d %d %d %d %d %d %d %d %d %d %.4f\n", std::get<0>(k), std::get<1>(k),
                  std::get<2>(k), std::get<3>(k), std::get<4>(k), std::get<5>(k), l.pt, l.occ,
-                 l.split, ms);
+                 l.split, l.tc, ms);
     std::fclose(f);
 }
 
@@ -104,10 +109,12 @@ size_t nu_tune_partial_bytes(const NuPlan &p, bool adj) {
 }
 
 bool nu_tuned_lookup(const NuPlan &p, bool adj, NuLaunch *out) {
+    if (!tuning_enabled()) return false;  // IMP_AUTOTUNE=0: default shapes only
     std::lock_guard<std::mutex> g(g_mu);
     load_locked();
     auto it = g_cache.find(key_of(p, adj));
     if (it == g_cache.end()) return false;
+    if (it->second.tc && !nu_tc_enabled()) return false;
     *out = it->second;
     return true;
 }
@@ -131,37 +138,49 @@ cudaError_t nu_autotune(const NuPlan &p, bool adj, const float2 *tdata, float2 *
     }
     float best = 1e30f;
     NuLaunch best_l = *out;
+    std::vector<NuLaunch> cands;
     for (int pt : pts_for(p.CG))
         for (int occ : {4, 6})
             for (int s = 1; s <= kMaxSplit; s *= 2) {
-                if (!nu_split_ok(n_theirs, s)) continue;
                 NuLaunch l;
                 l.pt = pt;
                 l.occ = occ;
                 l.split = s;
-                const size_t need = adj ? nu_adj_partial_bytes(p, l) : nu_fwd_partial_bytes(p, l);
-                if (need > part_bytes) continue;
-                auto run = [&]() {
-                    return adj ? nu_adjoint_partials(p, l, tdata, part, dev_err, st)
-                               : nu_forward_partials(p, l, tdata, part, dev_err, st);
-                };
-                if ((e = run()) != cudaSuccess) break;  // warm-up
-                float ms_min = 1e30f;
-                for (int rep = 0; rep < 2; ++rep) {
-                    cudaEventRecord(e0, st);
-                    if ((e = run()) != cudaSuccess) break;
-                    cudaEventRecord(e1, st);
-                    cudaEventSynchronize(e1);
-                    float ms = 0.f;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    ms_min = ms < ms_min ? ms : ms_min;
-                }
-                if (e != cudaSuccess) break;
-                if (ms_min < best) {
-                    best = ms_min;
-                    best_l = l;
-                }
+                cands.push_back(l);
             }
+    const int n_ours = adj ? p.Npad : p.Mpad;
+    if (nu_tc_enabled() && nu_tc_supported(p.CG) && n_ours % kTcRows == 0)
+        for (int s = 1; s <= kMaxSplit; s *= 2) {
+            NuLaunch l;
+            l.tc = 1;
+            l.split = s;
+            cands.push_back(l);
+        }
+    for (const NuLaunch &l : cands) {
+        if (!nu_split_ok(n_theirs, l.split)) continue;
+        const size_t need = adj ? nu_adj_partial_bytes(p, l) : nu_fwd_partial_bytes(p, l);
+        if (need > part_bytes) continue;
+        auto run = [&]() {
+            return adj ? nu_adjoint_partials(p, l, tdata, part, dev_err, st)
+                       : nu_forward_partials(p, l, tdata, part, dev_err, st);
+        };
+        if ((e = run()) != cudaSuccess) break;  // warm-up
+        float ms_min = 1e30f;
+        for (int rep = 0; rep < 2; ++rep) {
+            cudaEventRecord(e0, st);
+            if ((e = run()) != cudaSuccess) break;
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms_min = ms < ms_min ? ms : ms_min;
+        }
+        if (e != cudaSuccess) break;
+        if (ms_min < best) {
+            best = ms_min;
+            best_l = l;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (e != cudaSuccess) return e;

@@ -267,13 +267,18 @@ def test_cli_mgpu_matches_single_gpu(pkg, tmp_path):
     assert np.max(np.abs(outs[0] - outs[1])) <= 2e-6 + 1e-5 * np.max(np.abs(outs[0]))
 
 
-def test_batch_with_uneven_trajectories(pkg, ctx, synth):
+def test_batch_with_uneven_trajectories(pkg, ctx, synth, monkeypatch):
     """imp_bruteforce_batch: slices with their own spirals of different lengths
     and their own field maps, solved in lockstep by one batched solver; each
     slice matches the single-slice call on its own trajectory to 1e-5 (the
     batched launches split the FP32 partial sums and the FP64 block partials
-    differently) and stays within 1e-4 of the FP64 oracle."""
+    differently) and stays within 1e-4 of the FP64 oracle.  The single-slice
+    calls take the default launch shape (no autotuning), so that both solves
+    run the same NUDFT kernel: TV reweighting amplifies the 1e-7-level
+    difference between the tensor-core and CUDA-core kernels about a
+    hundredfold."""
     from gpu_util import gpu_recon
+    monkeypatch.setenv("IMP_AUTOTUNE", "0")
     rng = np.random.default_rng(17)
     n, C = 32, 2
     ix, iy, iz = synth.grid_positions(n, n, 1)
