@@ -383,8 +383,8 @@ cudaError_t BfBatch::setup(const BfConfig &cfg, int S, const int *k_off, const f
     // one launch shape for every slice
     fwd_ = nu_default_launch(plan_, false);
     adj_ = nu_default_launch(plan_, true);
-    const int fwd_rows = fwd_.tc ? kTcRows : kNT * fwd_.pt;
-    const int adj_rows = adj_.tc ? kTcRows : kNT * adj_.pt;
+    const int fwd_rows = fwd_.tc ? nu_tc_rows(CG) : kNT * fwd_.pt;
+    const int adj_rows = adj_.tc ? nu_tc_rows(CG) : kNT * adj_.pt;
     fwd_.split = batch_split((long long)(mpad_total_ / fwd_rows) * G, std::vector<int>{Npad},
                              fwd_.tc != 0);
     adj_.split = batch_split((long long)(Npad / adj_rows) * G * S, mpad_, adj_.tc != 0);

@@ -422,11 +422,15 @@ bool nu_shape_supported(int CG, int pt) {
            (CG == 4 && (pt == 2 || pt == 4)) || (CG == 8 && pt == 2);
 }
 
+// Coils per group.  Above 8 coils the tensor-core kernel takes groups of 16
+// or 32 (one phase per pair for all of them); IMP_NUDFT_TC=0 keeps groups of
+// at most 8 for the CUDA-core kernel.
 static int choose_cg(int C) {
     if (C <= 1) return 1;
     if (C <= 2) return 2;
     if (C <= 4) return 4;
-    return 8;
+    if (C <= 8 || !nu_tc_enabled()) return 8;
+    return C <= 16 ? 16 : 32;
 }
 
 static int round_up(int a, int b) { return (a + b - 1) / b * b; }
@@ -436,10 +440,11 @@ NuLaunch nu_default_launch(const NuPlan &p, bool adj) {
     l.pt = p.CG >= 8 ? 2 : 4;
     const int n_ours = adj ? p.Npad : p.Mpad;
     const int n_theirs = adj ? p.Mpad : p.Npad;
-    if (nu_tc_forced() && nu_tc_supported(p.CG) && n_ours % kTcRows == 0) {
+    const bool simt = nu_shape_supported(p.CG, p.CG >= 8 ? 2 : 4);
+    if ((nu_tc_forced() || !simt) && nu_tc_supported(p.CG) && n_ours % nu_tc_rows(p.CG) == 0) {
         // one block per SM: about eight waves of blocks, whole tiles per split
         l.tc = 1;
-        const long blocks = (long)(n_ours / kTcRows) * p.G;
+        const long blocks = (long)(n_ours / nu_tc_rows(p.CG)) * p.G;
         int split = 1;
         while (blocks * split < 148L * 8 && split < 64 && nu_split_ok(n_theirs, split * 2) &&
                n_theirs / (split * 2) >= 4 * kTile)

@@ -29,8 +29,6 @@ struct NuLaunch {
     int tc = 0;     // 1: tensor-core kernel (nudft_tc.cu; pt and occ unused)
 };
 
-constexpr int kTcRows = 256;  // "ours" rows per block of the tensor-core kernel
-
 struct NuPlan {
     int M = 0, N = 0, C = 0;     // samples, voxels, coils
     int CG = 1, G = 1;           // coils per group, groups (CG * G >= C)
@@ -123,12 +121,15 @@ bool nu_split_ok(int n_theirs, int split);
 
 // Tensor-core kernel (nudft_tc.cu): same partial-sum layouts as
 // nu_forward_partials / nu_adjoint_partials / nu_partials_batch; coil groups
-// of 1, 2, 4 or 8.  It is an autotuner candidate unless IMP_NUDFT_TC=0
-// (nu_tc_enabled), and the default launch shape when IMP_NUDFT_TC=1
-// (nu_tc_forced).
+// of 1, 2, 4, 8, 16 or 32.  It is an autotuner candidate unless
+// IMP_NUDFT_TC=0 (nu_tc_enabled), the default launch shape when
+// IMP_NUDFT_TC=1 (nu_tc_forced), and the only kernel for coil groups of 16
+// and 32 (plans of more than 8 coils, unless IMP_NUDFT_TC=0).
 bool nu_tc_supported(int CG);
 bool nu_tc_enabled();
 bool nu_tc_forced();
+// "ours" rows per block of the tensor-core kernel for coil groups of CG.
+int nu_tc_rows(int CG);
 cudaError_t nu_partials_tc(const NuPlan &p, const NuLaunch &l, bool adj, const float2 *tdata,
                            float2 *out, unsigned *dev_err, cudaStream_t st);
 cudaError_t nu_partials_tc_batch(const NuPlan &p, const NuLaunch &l, bool adj, int S,

@@ -11,8 +11,9 @@
 // phase and e = (cos, sin) of the angle once per row, split each component
 // into a TF32 head and tail (v = hi + lo, hi = v rounded to TF32) and store
 //     A[row][4j .. 4j+3] = (cos_hi, sin_hi, cos_lo, sin_lo)
-// into tensor memory.  The "theirs" data d_c (per coil) is expanded once per
-// tile into the B operand (shared memory, K-major, 128-byte swizzle), with
+// into tensor memory.  The "theirs" data d_c (per coil) is expanded chunk by
+// chunk (16 elements) by the same producer threads into the B operand (shared
+// memory, K-major, 128-byte swizzle), with
 // rows n of the N = NN accumulator columns
 //     n = 2c     (re, head):  ( dx_hi,  dy_hi,  dx_hi,  dy_hi)
 //     n = 2c + 1 (im, head):  ( dy_hi, -dx_hi,  dy_hi, -dx_hi)
@@ -29,7 +30,7 @@
 //                     the "theirs" share w / 4 (of H) of every chunk; groups
 //                     0 .. PT-1 also drain the accumulators of row tile
 //                     (w / 4) and write the partial sums
-//   warp 4H           bulk loads of the "theirs" tiles; B expansion
+//   warp 4H           bulk loads of the "theirs" tiles
 //   warp 4H + 1       tensor-memory allocation and the MMA issue (lane 0)
 // Every mbarrier wait is bounded; on expiry DEV_ERR_TIMEOUT is raised and the
 // kernel runs to its end.
@@ -90,16 +91,6 @@ __host__ __device__ constexpr uint32_t tc_idesc(int N) {
     return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | (8u << 24);
 }
 
-__device__ __forceinline__ void tc_st16(uint32_t taddr, const uint32_t *v) {
-    asm volatile(
-        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
-        "%13,%14,%15,%16};" ::"r"(taddr),
-        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
-        "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
-        "r"(v[15])
-        : "memory");
-}
-
 __device__ __forceinline__ void tc_st32(uint32_t taddr, const uint32_t *v) {
     asm volatile(
         "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,"
@@ -137,31 +128,40 @@ __device__ __forceinline__ void tc_fence_after_sync() {
 // Compile-time shape of one instantiation.
 template <int CG, int PT, int H>
 struct TcShape {
-    static constexpr int NN = CG <= 4 ? 16 : 32;      // accumulator columns
+    static constexpr int NN = CG <= 4 ? 16 : 4 * CG;  // accumulator columns
     static constexpr int HALF = NN / 2;               // tail columns start here
-    static constexpr int KC = 16;                     // "theirs" per A chunk
+    static constexpr int CSLOT = HALF / 2;            // coil slots (CG, or 4 when CG < 4)
+    static constexpr int KC = 16;                     // "theirs" per chunk
     static constexpr int JPW = KC / H;                // "theirs" per producer warp per chunk
     static constexpr int CHUNKS = kTile / KC;         // chunks per "theirs" tile
     static constexpr int ACOLS = 4 * KC;              // A columns per row tile per chunk
     static constexpr int NB = 2;                      // A buffers
+    static constexpr int NBB = NB;                    // B chunk buffers (paired with A's)
     static constexpr int DCOLS = 2 * PT * NN;         // two accumulator sets
     static constexpr int USED = DCOLS + NB * PT * ACOLS;
     static constexpr int TMEM = USED <= 32 ? 32 : USED <= 64 ? 64 : USED <= 128 ? 128
                                 : USED <= 256 ? 256 : 512;
     static constexpr int ATOM = NN * 128;             // one 32-K atom of B
-    static constexpr int BTILE = (kTile / 8) * ATOM;  // B of one "theirs" tile
+    static constexpr int BCHUNK = 2 * ATOM;           // B of one chunk (64 K values)
     static constexpr int WARPS = 4 * H + 2;
     static constexpr int THREADS = 32 * WARPS;
     static constexpr int PROD = 4 * H;
     static constexpr int SCOLS = 4 * JPW;             // A columns per producer store
-    static constexpr int DT = (PT + H - 1) / H;       // row tiles a producer drains
+    // Accumulator drain: with PT == H each producer group g drains row tile g
+    // (all NN columns); with PT == 1 and H == 2 group g drains the coils
+    // [g CG / 2, (g + 1) CG / 2) of the single row tile (head and tail
+    // columns), and the adjoint's coil sum is completed across the groups.
+    static constexpr bool CSPLIT = PT == 1;
+    static constexpr int DCOL_N = CSPLIT ? CG : NN;   // columns drained per range
+    static constexpr int NACC = CSPLIT ? 2 * CG : NN; // accumulators per producer thread
     static_assert(USED <= 512, "tensor memory");
-    static_assert(SCOLS == 16 || SCOLS == 32, "16- or 32-column stores");
-    static_assert(PT % H == 0 || H % PT == 0, "row tiles spread evenly over producer groups");
+    static_assert(SCOLS == 32, "one 32-column store per row tile and chunk");
+    static_assert(PT == H || (PT == 1 && H == 2 && CG >= 16), "drain assignment");
     static_assert(ACOLS == 64, "a chunk spans two 32-K atoms of B");
-    // dynamic shared memory: B[2] (1024-aligned) | geo[2] | dat[2]
-    static constexpr size_t SMEM = 1024 + 2 * (size_t)BTILE + 2 * kTile * sizeof(double4) +
-                                   2 * (size_t)kTile * CG * sizeof(float2);
+    static_assert(NN <= 256, "one MMA covers all accumulator columns");
+    // dynamic shared memory: B ring (1024-aligned) | geo[2] | dat[2] | red[128]
+    static constexpr size_t SMEM = 1024 + NBB * (size_t)BCHUNK + 2 * kTile * sizeof(double4) +
+                                   2 * (size_t)kTile * CG * sizeof(float2) + 128 * sizeof(float2);
 };
 
 template <int CG, int PT, int H, bool USEZ, bool ADJ, bool BATCH>
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
                unsigned *err, const NuSlice *__restrict__ sl, int n_groups) {
     using S = TcShape<CG, PT, H>;
     extern __shared__ unsigned char smraw[];
-    __shared__ __align__(8) uint64_t full[2], tempty[2], bfull[2], bempty[2];
+    __shared__ __align__(8) uint64_t full[2], tempty[2];
     __shared__ __align__(8) uint64_t afull[S::NB], aempty[S::NB], dfull[2], ddone[2];
     __shared__ uint32_t tmem_sh;
 
@@ -200,9 +200,11 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
     constexpr unsigned kDatBytes = kTile * CG * sizeof(float2);
 
     unsigned char *sm = smraw + ((1024u - (smem_u32(smraw) & 1023u)) & 1023u);
-    unsigned char *s_b = sm;                                                  // [2][BTILE]
-    double4 *s_geo = reinterpret_cast<double4 *>(sm + 2 * S::BTILE);          // [2][kTile]
-    float2 *s_dat = reinterpret_cast<float2 *>(sm + 2 * S::BTILE + 2 * kGeoBytes);  // [2][kTile*CG]
+    unsigned char *s_b = sm;                                          // [NBB][BCHUNK]
+    unsigned char *s_rest = sm + S::NBB * S::BCHUNK;
+    double4 *s_geo = reinterpret_cast<double4 *>(s_rest);             // [2][kTile]
+    float2 *s_dat = reinterpret_cast<float2 *>(s_rest + 2 * kGeoBytes);  // [2][kTile * CG]
+    float2 *s_red = reinterpret_cast<float2 *>(s_rest + 2 * kGeoBytes + 2 * kDatBytes);  // [128]
 
     if (warp == S::PROD + 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -215,8 +217,6 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
         for (int i = 0; i < 2; ++i) {
             mbar_init(&full[i], 1);
             mbar_init(&tempty[i], S::PROD);
-            mbar_init(&bfull[i], 1);
-            mbar_init(&bempty[i], 1);
             mbar_init(&dfull[i], 1);
             mbar_init(&ddone[i], S::PROD);
         }
@@ -246,29 +246,59 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
             oz[p] = q.z;
             ow[p] = q.w;
         }
-        constexpr int DT = S::DT;  // row tiles this thread drains: grp, grp + H, ... (< PT)
-        float acc[DT][S::NN];
+        // drained row tile and accumulator column ranges of this producer group
+        const int dtile = S::CSPLIT ? 0 : grp;
+        const int head0 = S::CSPLIT ? grp * CG : 0;          // first head column
+        const int tail0 = S::CSPLIT ? S::HALF + grp * CG : 0;  // first tail column (CSPLIT)
+        const bool drains = dtile < PT;
+        float acc[S::NACC];
 #pragma unroll
-        for (int i = 0; i < DT; ++i)
-#pragma unroll
-            for (int n = 0; n < S::NN; ++n) acc[i][n] = 0.f;
+        for (int n = 0; n < S::NACC; ++n) acc[n] = 0.f;
         const uint32_t tlane = tmem + ((uint32_t)(quad * 32) << 16);
+        // B operand of one chunk from its KC "theirs" data records (all producer
+        // threads; items (sample jc, coil slot cc), 16 consecutive threads take
+        // the 16 samples of one coil: conflict-free 16-byte stores)
+        const int ptid = warp * 32 + lane;
+        auto expand_b = [&](unsigned char *bt, const float2 *dat) {
+#pragma unroll 1
+            for (int it = ptid; it < S::KC * S::CSLOT; it += S::PROD * 32) {
+                const int jc = it & (S::KC - 1), cc = it / S::KC;
+                unsigned char *atom = bt + (jc >> 3) * S::ATOM;
+                const unsigned chunk = (unsigned)(jc & 7);
+                auto put = [&](int n, float a0, float a1, float a2, float a3) {
+                    const unsigned off = (unsigned)(n >> 3) * 1024 + (unsigned)(n & 7) * 128 +
+                                         ((chunk ^ (unsigned)(n & 7)) << 4);
+                    *reinterpret_cast<float4 *>(atom + off) = make_float4(a0, a1, a2, a3);
+                };
+                float xh = 0.f, yh = 0.f, xl = 0.f, yl = 0.f;
+                if (cc < CG) {
+                    const float2 d = dat[jc * CG + cc];
+                    xh = __uint_as_float(tf32_rna(d.x));
+                    yh = __uint_as_float(tf32_rna(d.y));
+                    xl = __uint_as_float(tf32_rna(d.x - xh));  // tail rounded, not truncated
+                    yl = __uint_as_float(tf32_rna(d.y - yh));
+                }
+                put(2 * cc, xh, yh, xh, yh);
+                put(2 * cc + 1, yh, -xh, yh, -xh);
+                put(S::HALF + 2 * cc, xl, yl, 0.f, 0.f);
+                put(S::HALF + 2 * cc + 1, yl, -xl, 0.f, 0.f);
+            }
+        };
         auto drain = [&](int t) {  // accumulators of tile t into acc
             const int b = t & 1;
-            tc_wait(&dfull[b], (unsigned)(t >> 1) & 1, ok);
+            tc_wait<20>(&dfull[b], (unsigned)(t >> 1) & 1, ok);
             tc_fence_after_sync();
+            if (drains) {
+                const uint32_t dcol = tlane + (uint32_t)((b * PT + dtile) * S::NN);
 #pragma unroll
-            for (int i = 0; i < DT; ++i) {
-                const int p = grp + i * H;
-                if (p >= PT) break;
-                const uint32_t dcol = (uint32_t)((b * PT + p) * S::NN);
+                for (int r = 0; r < (S::CSPLIT ? 2 : 1); ++r)
 #pragma unroll
-                for (int n0 = 0; n0 < S::NN; n0 += 16) {
-                    float f[16];
-                    tc_ld16(tlane + dcol + n0, f);
+                    for (int n0 = 0; n0 < S::DCOL_N; n0 += 16) {
+                        float f[16];
+                        tc_ld16(dcol + (uint32_t)((r ? tail0 : head0) + n0), f);
 #pragma unroll
-                    for (int n = 0; n < 16; ++n) acc[i][n0 + n] += f[n];
-                }
+                        for (int n = 0; n < 16; ++n) acc[r * S::DCOL_N + n0 + n] += f[n];
+                    }
             }
             tc_fence_before_sync();
             __syncwarp();
@@ -278,13 +308,15 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
         for (int t = 0; t < ntiles; ++t) {
             const int s = t & 1;
             if (t >= 2) drain(t - 2);
-            tc_wait(&full[s], (unsigned)(t >> 1) & 1, ok);
+            tc_wait<20>(&full[s], (unsigned)(t >> 1) & 1, ok);
             const double4 *geo = s_geo + s * kTile;
 #pragma unroll 1
             for (int c = 0; c < S::CHUNKS; ++c, ++ci) {
                 const int ab = ci % S::NB;
-                if (ci >= S::NB) tc_wait(&aempty[ab], (unsigned)(ci / S::NB - 1) & 1, ok);
+                // A buffer ab and B buffer ab are free once chunk ci - NB's MMAs are done
+                if (ci >= S::NB) tc_wait<20>(&aempty[ab], (unsigned)(ci / S::NB - 1) & 1, ok);
                 tc_fence_after_sync();
+                expand_b(s_b + ab * S::BCHUNK, s_dat + s * kTile * CG + c * S::KC * CG);
                 uint32_t v[PT][S::SCOLS];
 #pragma unroll
                 for (int jj = 0; jj < S::JPW; ++jj) {
@@ -312,12 +344,10 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
                 for (int p = 0; p < PT; ++p) {
                     const uint32_t ta =
                         tlane + (uint32_t)(S::DCOLS + (ab * PT + p) * S::ACOLS + grp * S::SCOLS);
-                    if constexpr (S::SCOLS == 32)
-                        tc_st32(ta, v[p]);
-                    else
-                        tc_st16(ta, v[p]);
+                    tc_st32(ta, v[p]);
                 }
                 asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+                fence_proxy_async_smem();  // this thread's B stores, for the MMA
                 tc_fence_before_sync();
                 __syncwarp();
                 if (lane == 0) tc_arrive(&afull[ab]);
@@ -329,79 +359,57 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
 
         // ------------------------------ partial sums -----------------------------
         const int G = BATCH ? n_groups : (int)gridDim.z;
+        const int e = blockIdx.x * (128 * PT) + dtile * 128 + row;
+        constexpr int NC = S::CSPLIT ? CG / 2 : CG;  // coils in this thread's accumulators
+        const int c0 = S::CSPLIT ? grp * NC : 0;     // first of them
+        const int hoff = S::CSPLIT ? S::DCOL_N : S::HALF;  // tail offset inside acc
+        if (!ADJ) {
+            if (drains) {
+                float2 *o = out + ((size_t)(split * G + g) * n_ours_pad + e) * CG + c0;
 #pragma unroll
-        for (int i = 0; i < DT; ++i) {
-            if (grp + i * H >= PT) break;
-            const int e = blockIdx.x * (128 * PT) + (grp + i * H) * 128 + row;
-            float re[CG], im[CG];
-#pragma unroll
-            for (int c = 0; c < CG; ++c) {
-                re[c] = acc[i][2 * c] + acc[i][S::HALF + 2 * c];
-                im[c] = acc[i][2 * c + 1] + acc[i][S::HALF + 2 * c + 1];
+                for (int c = 0; c < NC; ++c)
+                    o[c] = make_float2(acc[2 * c] + acc[hoff + 2 * c],
+                                       acc[2 * c + 1] + acc[hoff + 2 * c + 1]);
             }
-            if (!ADJ) {
-                float2 *o = out + ((size_t)(split * G + g) * n_ours_pad + e) * CG;
+        } else {
+            float zr = 0.f, zi = 0.f;
+            if (drains) {
+                const float2 *sv = sens + ((size_t)g * n_ours_pad + e) * CG + c0;
 #pragma unroll
-                for (int c = 0; c < CG; ++c) o[c] = make_float2(re[c], im[c]);
-            } else {
-                const float2 *sv = sens + ((size_t)g * n_ours_pad + e) * CG;
-                float zr = 0.f, zi = 0.f;
-#pragma unroll
-                for (int c = 0; c < CG; ++c) {
+                for (int c = 0; c < NC; ++c) {
+                    const float re = acc[2 * c] + acc[hoff + 2 * c];
+                    const float im = acc[2 * c + 1] + acc[hoff + 2 * c + 1];
                     const float2 w = sv[c];
-                    zr += w.x * re[c] + w.y * im[c];
-                    zi += w.x * im[c] - w.y * re[c];
+                    zr += w.x * re + w.y * im;
+                    zi += w.x * im - w.y * re;
                 }
+            }
+            if constexpr (S::CSPLIT) {
+                // coil sum across the two producer groups (producer warps only)
+                if (grp == 1) s_red[row] = make_float2(zr, zi);
+                asm volatile("bar.sync 1, %0;" ::"n"(S::PROD * 32) : "memory");
+                if (grp == 0) {
+                    const float2 o1 = s_red[row];
+                    out[(size_t)(split * G + g) * n_ours_pad + e] =
+                        make_float2(zr + o1.x, zi + o1.y);
+                }
+            } else if (drains) {
                 out[(size_t)(split * G + g) * n_ours_pad + e] = make_float2(zr, zi);
             }
         }
     } else if (warp == S::PROD) {
-        // ------------------------ loads and B expansion --------------------------
-        for (int t = 0; t < ntiles; ++t) {
-            const int s = t & 1;
-            if (t >= 2) tc_wait<256>(&tempty[s], (unsigned)((t - 2) >> 1) & 1, ok);
-            if (lane == 0) {
+        // ------------------------------ bulk loads ------------------------------
+        if (lane == 0)
+            for (int t = 0; t < ntiles; ++t) {
+                const int s = t & 1;
+                if (t >= 2) tc_wait<256>(&tempty[s], (unsigned)((t - 2) >> 1) & 1, ok);
                 fence_proxy_async_smem();
                 mbar_arrive_expect_tx(&full[s], kGeoBytes + kDatBytes);
                 bulk_g2s(s_geo + s * kTile, gsrc + (size_t)t * kTile, kGeoBytes, &full[s]);
                 bulk_g2s(s_dat + s * kTile * CG, dsrc + (size_t)t * kTile * CG, kDatBytes,
                          &full[s]);
             }
-            __syncwarp();
-            tc_wait<256>(&full[s], (unsigned)(t >> 1) & 1, ok);
-            if (t >= 2) tc_wait<256>(&bempty[s], (unsigned)((t - 2) >> 1) & 1, ok);
-            tc_fence_after_sync();
-            unsigned char *bt = s_b + s * S::BTILE;
-            const float2 *dat = s_dat + s * kTile * CG;
-#pragma unroll 1
-            for (int j = lane; j < kTile; j += 32) {
-                unsigned char *atom = bt + (j >> 3) * S::ATOM;
-                const unsigned chunk = (unsigned)(j & 7);
-                auto put = [&](int n, float a0, float a1, float a2, float a3) {
-                    const unsigned off = (unsigned)(n >> 3) * 1024 + (unsigned)(n & 7) * 128 +
-                                         ((chunk ^ (unsigned)(n & 7)) << 4);
-                    *reinterpret_cast<float4 *>(atom + off) = make_float4(a0, a1, a2, a3);
-                };
-#pragma unroll
-                for (int c = 0; c < S::HALF / 2; ++c) {
-                    float xh = 0.f, yh = 0.f, xl = 0.f, yl = 0.f;
-                    if (c < CG) {
-                        const float2 d = dat[j * CG + c];
-                        xh = __uint_as_float(tf32_rna(d.x));
-                        yh = __uint_as_float(tf32_rna(d.y));
-                        xl = __uint_as_float(tf32_rna(d.x - xh));  // tail rounded, not truncated
-                        yl = __uint_as_float(tf32_rna(d.y - yh));
-                    }
-                    put(2 * c, xh, yh, xh, yh);
-                    put(2 * c + 1, yh, -xh, yh, -xh);
-                    put(S::HALF + 2 * c, xl, yl, 0.f, 0.f);
-                    put(S::HALF + 2 * c + 1, yl, -xl, 0.f, 0.f);
-                }
-            }
-            fence_proxy_async_smem();
-            __syncwarp();
-            if (lane == 0) tc_arrive(&bfull[s]);
-        }
+        __syncwarp();
     } else {
         // ------------------------------- MMA issue -------------------------------
         if (lane == 0) {
@@ -410,14 +418,13 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
             int ci = 0;
             for (int t = 0; t < ntiles; ++t) {
                 const int s = t & 1;
-                tc_wait<32>(&bfull[s], (unsigned)(t >> 1) & 1, ok);
                 if (t >= 2) tc_wait<32>(&ddone[s], (unsigned)((t - 2) >> 1) & 1, ok);
                 for (int c = 0; c < S::CHUNKS; ++c, ++ci) {
                     const int ab = ci % S::NB;
                     tc_wait<32>(&afull[ab], (unsigned)(ci / S::NB) & 1, ok);
                     tc_fence_after_sync();
-                    // chunk c covers B atoms 2c, 2c + 1 (S::ACOLS = 64 K values)
-                    const uint64_t bd = tc_bdesc(sb0 + s * S::BTILE + c * 2 * S::ATOM);
+                    // the chunk's B: atoms 0, 1 of buffer ab (S::ACOLS = 64 K values)
+                    const uint64_t bd = tc_bdesc(sb0 + ab * S::BCHUNK);
                     const uint32_t dbase = tmem + (uint32_t)(s * PT * S::NN);
                     const uint32_t abase = tmem + (uint32_t)(S::DCOLS + ab * PT * S::ACOLS);
                     const uint32_t first = c > 0 ? 1u : 0u;
@@ -440,7 +447,6 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
                     tc_commit(&aempty[ab]);
                 }
                 tc_commit(&dfull[s]);
-                tc_commit(&bempty[s]);
             }
         }
         __syncwarp();
@@ -476,7 +482,7 @@ template <int CG, bool ADJ, bool BATCH>
 cudaError_t launch_tc_z(const NuPlan &p, dim3 grid, const double4 *ours, const double4 *theirs,
                         const float2 *tdata, float2 *out, int n_ours, int n_theirs,
                         int per_split, unsigned *err, const NuSlice *sl, cudaStream_t st) {
-    constexpr int PT = 2, H = 2;
+    constexpr int PT = CG >= 32 ? 1 : 2, H = 2;
     if (p.use_z)
         return launch_tc<CG, PT, H, true, ADJ, BATCH>(grid, ours, theirs, tdata, p.sens, out,
                                                       n_ours, n_theirs, per_split, err, sl, p.G,
@@ -502,6 +508,12 @@ cudaError_t launch_tc_cg(const NuPlan &p, dim3 grid, const double4 *ours, const 
         case 8:
             return launch_tc_z<8, ADJ, BATCH>(p, grid, ours, theirs, tdata, out, n_ours,
                                               n_theirs, per_split, err, sl, st);
+        case 16:
+            return launch_tc_z<16, ADJ, BATCH>(p, grid, ours, theirs, tdata, out, n_ours,
+                                               n_theirs, per_split, err, sl, st);
+        case 32:
+            return launch_tc_z<32, ADJ, BATCH>(p, grid, ours, theirs, tdata, out, n_ours,
+                                               n_theirs, per_split, err, sl, st);
         default:
             return cudaErrorInvalidConfiguration;
     }
@@ -509,14 +521,19 @@ cudaError_t launch_tc_cg(const NuPlan &p, dim3 grid, const double4 *ours, const 
 
 }  // namespace
 
-bool nu_tc_supported(int CG) { return CG == 1 || CG == 2 || CG == 4 || CG == 8; }
+bool nu_tc_supported(int CG) {
+    return CG == 1 || CG == 2 || CG == 4 || CG == 8 || CG == 16 || CG == 32;
+}
+
+int nu_tc_rows(int CG) { return CG >= 32 ? 128 : 256; }
 
 cudaError_t nu_partials_tc(const NuPlan &p, const NuLaunch &l, bool adj, const float2 *tdata,
                            float2 *out, unsigned *err, cudaStream_t st) {
     const int n_ours = adj ? p.Npad : p.Mpad;
     const int n_theirs = adj ? p.Mpad : p.Npad;
-    if (!nu_split_ok(n_theirs, l.split) || n_ours % kTcRows) return cudaErrorInvalidConfiguration;
-    const dim3 grid(n_ours / kTcRows, l.split, p.G);
+    const int rows = nu_tc_rows(p.CG);
+    if (!nu_split_ok(n_theirs, l.split) || n_ours % rows) return cudaErrorInvalidConfiguration;
+    const dim3 grid(n_ours / rows, l.split, p.G);
     const double4 *ours = adj ? p.vgeo : p.kgeo;
     const double4 *theirs = adj ? p.kgeo : p.vgeo;
     const int per_split = n_theirs / l.split;
@@ -530,8 +547,9 @@ cudaError_t nu_partials_tc_batch(const NuPlan &p, const NuLaunch &l, bool adj, i
                                  int max_ours, const NuSlice *d_slices, const double4 *ours,
                                  const double4 *theirs, const float2 *tdata, float2 *out,
                                  unsigned *err, cudaStream_t st) {
-    if ((long long)S * p.G > 65535 || max_ours % kTcRows) return cudaErrorInvalidConfiguration;
-    const dim3 grid(max_ours / kTcRows, l.split, S * p.G);
+    const int rows = nu_tc_rows(p.CG);
+    if ((long long)S * p.G > 65535 || max_ours % rows) return cudaErrorInvalidConfiguration;
+    const dim3 grid(max_ours / rows, l.split, S * p.G);
     return adj ? launch_tc_cg<true, true>(p, grid, ours, theirs, tdata, out, 0, 0, 0, err,
                                           d_slices, st)
                : launch_tc_cg<false, true>(p, grid, ours, theirs, tdata, out, 0, 0, 0, err,

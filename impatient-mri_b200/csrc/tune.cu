@@ -149,7 +149,7 @@ cudaError_t nu_autotune(const NuPlan &p, bool adj, const float2 *tdata, float2 *
                 cands.push_back(l);
             }
     const int n_ours = adj ? p.Npad : p.Mpad;
-    if (nu_tc_enabled() && nu_tc_supported(p.CG) && n_ours % kTcRows == 0)
+    if (nu_tc_enabled() && nu_tc_supported(p.CG) && n_ours % nu_tc_rows(p.CG) == 0)
         for (int s = 1; s <= kMaxSplit; s *= 2) {
             NuLaunch l;
             l.tc = 1;

@@ -57,8 +57,10 @@ def check(a, b, ref):
     assert not np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("C", [1, 2, 3, 4, 8, 9])
+@pytest.mark.parametrize("C", [1, 2, 3, 4, 8, 9, 16, 20, 32, 40])
 def test_coil_groups_2d(pkg, ctx, synth, C):
+    """Coil groups of 1, 2, 4, 8 (both kernels), 16 and 32 (tensor-core kernel
+    only; with IMP_NUDFT_TC=0 the plan takes groups of 8)."""
     from gpu_util import gpu_ft, gpu_ift
     c = case_nd(synth, 32, 32, 1, C, 1000, seed=40 + C)
     rng = np.random.default_rng(C)
@@ -70,7 +72,7 @@ def test_coil_groups_2d(pkg, ctx, synth, C):
     check(a, b, oracle.ift(d, c, use_z=0))
 
 
-@pytest.mark.parametrize("C", [1, 4])
+@pytest.mark.parametrize("C", [1, 4, 32])
 def test_3d_with_field_map(pkg, ctx, synth, C):
     from gpu_util import gpu_ft, gpu_ift
     c = case_nd(synth, 16, 16, 8, C, 3000, seed=50 + C)
