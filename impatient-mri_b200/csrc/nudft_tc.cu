@@ -52,7 +52,9 @@ __device__ __forceinline__ uint32_t tf32_rna(float v) {
 }
 
 // Bounded wait: at most 2^20 tries, SLEEP ns apart (the loader and MMA warps
-// back off so that their polling takes few issue slots from the producers).
+// back off so that their polling takes few issue slots from the producers;
+// the producers, about four times slower per chunk than the MMAs, leave the
+// MMA warp that much slack).
 // After one expiry (ok == false) the thread stops waiting, so a broken
 // pipeline ends the launch after one timeout per thread.
 template <unsigned SLEEP = 0>
@@ -135,7 +137,9 @@ struct TcShape {
     static constexpr int JPW = KC / H;                // "theirs" per producer warp per chunk
     static constexpr int CHUNKS = kTile / KC;         // chunks per "theirs" tile
     static constexpr int ACOLS = 4 * KC;              // A columns per row tile per chunk
-    static constexpr int NB = 2;                      // A buffers
+    // A (and B) chunk buffers.  Three (where tensor memory holds them) measured
+    // slower: 32 coils 31.8 -> 82.5 ms per forward + adjoint pair.
+    static constexpr int NB = 2;
     static constexpr int NBB = NB;                    // B chunk buffers (paired with A's)
     static constexpr int DCOLS = 2 * PT * NN;         // two accumulator sets
     static constexpr int USED = DCOLS + NB * PT * ACOLS;
@@ -402,7 +406,7 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
         if (lane == 0)
             for (int t = 0; t < ntiles; ++t) {
                 const int s = t & 1;
-                if (t >= 2) tc_wait<256>(&tempty[s], (unsigned)((t - 2) >> 1) & 1, ok);
+                if (t >= 2) tc_wait<512>(&tempty[s], (unsigned)((t - 2) >> 1) & 1, ok);
                 fence_proxy_async_smem();
                 mbar_arrive_expect_tx(&full[s], kGeoBytes + kDatBytes);
                 bulk_g2s(s_geo + s * kTile, gsrc + (size_t)t * kTile, kGeoBytes, &full[s]);
@@ -418,10 +422,10 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
             int ci = 0;
             for (int t = 0; t < ntiles; ++t) {
                 const int s = t & 1;
-                if (t >= 2) tc_wait<32>(&ddone[s], (unsigned)((t - 2) >> 1) & 1, ok);
+                if (t >= 2) tc_wait<128>(&ddone[s], (unsigned)((t - 2) >> 1) & 1, ok);
                 for (int c = 0; c < S::CHUNKS; ++c, ++ci) {
                     const int ab = ci % S::NB;
-                    tc_wait<32>(&afull[ab], (unsigned)(ci / S::NB) & 1, ok);
+                    tc_wait<128>(&afull[ab], (unsigned)(ci / S::NB) & 1, ok);
                     tc_fence_after_sync();
                     // the chunk's B: atoms 0, 1 of buffer ab (S::ACOLS = 64 K values)
                     const uint64_t bd = tc_bdesc(sb0 + ab * S::BCHUNK);
