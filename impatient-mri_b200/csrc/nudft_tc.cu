@@ -37,6 +37,8 @@
 #include "nudft.cuh"
 #include "common.cuh"
 
+#include <atomic>
+
 namespace imp {
 
 namespace {
@@ -470,12 +472,17 @@ cudaError_t launch_tc(dim3 grid, const double4 *ours, const double4 *theirs, con
                       unsigned *err, const NuSlice *sl, int G, cudaStream_t st) {
     using S = TcShape<CG, PT, H>;
     auto k = k_nudft_tc<CG, PT, H, USEZ, ADJ, BATCH>;
-    static bool attr = false;  // per instantiation; set once per process
-    if (!attr) {
-        cudaError_t e =
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
+    // the shared-memory limit is set once per instantiation and device (-mgpu
+    // workers drive several devices from several threads)
+    static std::atomic<unsigned long long> attr_set{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (!bit || !(attr_set.load(std::memory_order_acquire) & bit)) {
+        e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM);
         if (e != cudaSuccess) return e;
-        attr = true;
+        attr_set.fetch_or(bit, std::memory_order_acq_rel);
     }
     k<<<grid, S::THREADS, S::SMEM, st>>>(ours, theirs, tdata, sens, out, n_ours, n_theirs,
                                          per_split, err, sl, G);
