@@ -139,8 +139,8 @@ struct TcShape {
     static constexpr int JPW = KC / H;                // "theirs" per producer warp per chunk
     static constexpr int CHUNKS = kTile / KC;         // chunks per "theirs" tile
     static constexpr int ACOLS = 4 * KC;              // A columns per row tile per chunk
-    // A (and B) chunk buffers.  Three (where tensor memory holds them) measured
-    // slower: 32 coils 31.8 -> 82.5 ms per forward + adjoint pair.
+    // A (and B) chunk buffers (a third, where tensor memory holds it, gave no
+    // measurable gain)
     static constexpr int NB = 2;
     static constexpr int NBB = NB;                    // B chunk buffers (paired with A's)
     static constexpr int DCOLS = 2 * PT * NN;         // two accumulator sets
@@ -165,9 +165,15 @@ struct TcShape {
     static_assert(PT == H || (PT == 1 && H == 2 && CG >= 16), "drain assignment");
     static_assert(ACOLS == 64, "a chunk spans two 32-K atoms of B");
     static_assert(NN <= 256, "one MMA covers all accumulator columns");
+    // "theirs" data rows in shared memory: CG float2 per element, padded by 16
+    // bytes from 8 coils up (one bulk copy per element), so that the B expansion's
+    // reads of 16 consecutive elements of one coil spread over the banks
+    static constexpr bool PADDAT = CG >= 8;
+    static constexpr int DROWF = PADDAT ? CG + 2 : CG;  // float2 per row
     // dynamic shared memory: B ring (1024-aligned) | geo[2] | dat[2] | red[128]
     static constexpr size_t SMEM = 1024 + NBB * (size_t)BCHUNK + 2 * kTile * sizeof(double4) +
-                                   2 * (size_t)kTile * CG * sizeof(float2) + 128 * sizeof(float2);
+                                   2 * (size_t)kTile * DROWF * sizeof(float2) +
+                                   128 * sizeof(float2);
 };
 
 template <int CG, int PT, int H, bool USEZ, bool ADJ, bool BATCH>
@@ -209,8 +215,9 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
     unsigned char *s_b = sm;                                          // [NBB][BCHUNK]
     unsigned char *s_rest = sm + S::NBB * S::BCHUNK;
     double4 *s_geo = reinterpret_cast<double4 *>(s_rest);             // [2][kTile]
-    float2 *s_dat = reinterpret_cast<float2 *>(s_rest + 2 * kGeoBytes);  // [2][kTile * CG]
-    float2 *s_red = reinterpret_cast<float2 *>(s_rest + 2 * kGeoBytes + 2 * kDatBytes);  // [128]
+    float2 *s_dat = reinterpret_cast<float2 *>(s_rest + 2 * kGeoBytes);  // [2][kTile][DROWF]
+    constexpr unsigned kDatSmem = kTile * S::DROWF * sizeof(float2);  // one tile's rows
+    float2 *s_red = reinterpret_cast<float2 *>(s_rest + 2 * kGeoBytes + 2 * kDatSmem);  // [128]
 
     if (warp == S::PROD + 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -278,7 +285,7 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
                 };
                 float xh = 0.f, yh = 0.f, xl = 0.f, yl = 0.f;
                 if (cc < CG) {
-                    const float2 d = dat[jc * CG + cc];
+                    const float2 d = dat[jc * S::DROWF + cc];
                     xh = __uint_as_float(tf32_rna(d.x));
                     yh = __uint_as_float(tf32_rna(d.y));
                     xl = __uint_as_float(tf32_rna(d.x - xh));  // tail rounded, not truncated
@@ -322,7 +329,7 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
                 // A buffer ab and B buffer ab are free once chunk ci - NB's MMAs are done
                 if (ci >= S::NB) tc_wait<20>(&aempty[ab], (unsigned)(ci / S::NB - 1) & 1, ok);
                 tc_fence_after_sync();
-                expand_b(s_b + ab * S::BCHUNK, s_dat + s * kTile * CG + c * S::KC * CG);
+                expand_b(s_b + ab * S::BCHUNK, s_dat + (s * kTile + c * S::KC) * S::DROWF);
                 uint32_t v[PT][S::SCOLS];
 #pragma unroll
                 for (int jj = 0; jj < S::JPW; ++jj) {
@@ -412,8 +419,15 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
                 fence_proxy_async_smem();
                 mbar_arrive_expect_tx(&full[s], kGeoBytes + kDatBytes);
                 bulk_g2s(s_geo + s * kTile, gsrc + (size_t)t * kTile, kGeoBytes, &full[s]);
-                bulk_g2s(s_dat + s * kTile * CG, dsrc + (size_t)t * kTile * CG, kDatBytes,
-                         &full[s]);
+                if constexpr (S::PADDAT) {
+                    for (int j = 0; j < kTile; ++j)  // CG * 8 bytes: a multiple of 16
+                        bulk_g2s(s_dat + (s * kTile + j) * S::DROWF,
+                                 dsrc + ((size_t)t * kTile + j) * CG, CG * sizeof(float2),
+                                 &full[s]);
+                } else {
+                    bulk_g2s(s_dat + s * kTile * CG, dsrc + (size_t)t * kTile * CG, kDatBytes,
+                             &full[s]);
+                }
             }
         __syncwarp();
     } else {
