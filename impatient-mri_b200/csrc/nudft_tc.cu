@@ -270,31 +270,43 @@ __global__ void __launch_bounds__(TcShape<CG, PT, H>::THREADS, 1)
         const uint32_t tlane = tmem + ((uint32_t)(quad * 32) << 16);
         // B operand of one chunk from its KC "theirs" data records (all producer
         // threads; items (sample jc, coil slot cc), 16 consecutive threads take
-        // the 16 samples of one coil: conflict-free 16-byte stores)
+        // the 16 samples of one coil: conflict-free 16-byte stores).  A thread's
+        // items and their offsets are the same in every chunk: computed once.
         const int ptid = warp * 32 + lane;
+        constexpr int NITEM = S::KC * S::CSLOT;
+        constexpr int NIT = (NITEM + S::PROD * 32 - 1) / (S::PROD * 32);
+        int it_dat[NIT];       // float2 index of the item's datum in a chunk's rows (-1: none)
+        unsigned it_off[NIT][4];  // byte offsets of its four B rows in a chunk buffer
+#pragma unroll
+        for (int i = 0; i < NIT; ++i) {
+            const int it = ptid + i * S::PROD * 32;
+            const int jc = it & (S::KC - 1), cc = it / S::KC;
+            const unsigned chunk = (unsigned)(jc & 7);
+            const unsigned atom = (unsigned)(jc >> 3) * S::ATOM;
+            const int rows[4] = {2 * cc, 2 * cc + 1, S::HALF + 2 * cc, S::HALF + 2 * cc + 1};
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const unsigned n = (unsigned)rows[r];
+                it_off[i][r] = atom + (n >> 3) * 1024 + (n & 7) * 128 + ((chunk ^ (n & 7)) << 4);
+            }
+            it_dat[i] = (it < NITEM && cc < CG) ? jc * S::DROWF + cc : (it < NITEM ? -2 : -1);
+        }
         auto expand_b = [&](unsigned char *bt, const float2 *dat) {
-#pragma unroll 1
-            for (int it = ptid; it < S::KC * S::CSLOT; it += S::PROD * 32) {
-                const int jc = it & (S::KC - 1), cc = it / S::KC;
-                unsigned char *atom = bt + (jc >> 3) * S::ATOM;
-                const unsigned chunk = (unsigned)(jc & 7);
-                auto put = [&](int n, float a0, float a1, float a2, float a3) {
-                    const unsigned off = (unsigned)(n >> 3) * 1024 + (unsigned)(n & 7) * 128 +
-                                         ((chunk ^ (unsigned)(n & 7)) << 4);
-                    *reinterpret_cast<float4 *>(atom + off) = make_float4(a0, a1, a2, a3);
-                };
+#pragma unroll
+            for (int i = 0; i < NIT; ++i) {
+                if (it_dat[i] == -1) continue;  // no item for this thread
                 float xh = 0.f, yh = 0.f, xl = 0.f, yl = 0.f;
-                if (cc < CG) {
-                    const float2 d = dat[jc * S::DROWF + cc];
+                if (it_dat[i] >= 0) {  // -2: a padding coil slot (zero rows)
+                    const float2 d = dat[it_dat[i]];
                     xh = __uint_as_float(tf32_rna(d.x));
                     yh = __uint_as_float(tf32_rna(d.y));
                     xl = __uint_as_float(tf32_rna(d.x - xh));  // tail rounded, not truncated
                     yl = __uint_as_float(tf32_rna(d.y - yh));
                 }
-                put(2 * cc, xh, yh, xh, yh);
-                put(2 * cc + 1, yh, -xh, yh, -xh);
-                put(S::HALF + 2 * cc, xl, yl, 0.f, 0.f);
-                put(S::HALF + 2 * cc + 1, yl, -xl, 0.f, 0.f);
+                *reinterpret_cast<float4 *>(bt + it_off[i][0]) = make_float4(xh, yh, xh, yh);
+                *reinterpret_cast<float4 *>(bt + it_off[i][1]) = make_float4(yh, -xh, yh, -xh);
+                *reinterpret_cast<float4 *>(bt + it_off[i][2]) = make_float4(xl, yl, 0.f, 0.f);
+                *reinterpret_cast<float4 *>(bt + it_off[i][3]) = make_float4(yl, -xl, 0.f, 0.f);
             }
         };
         auto drain = [&](int t) {  // accumulators of tile t into acc
