@@ -6,7 +6,9 @@
 // replaces ftGpuKernel / iftGpuKernel (kernels/ftGpu.cu:306-604, 756-1013) and
 // the coil loop of parallelFtGpu / parallelIftGpu (kernels/parImagingGpu.cu:92-152).
 //
-// Per CTA: PT accumulator tiles of 128 "ours" rows (tensor-memory lane = row).
+// Per CTA: PT accumulator tiles of 128 "ours" rows (tensor-memory lane = row);
+// PT = 2 for coil groups of up to 16, 1 for 32 (N = NN columns: 16 up to 4
+// coils, else 4 per coil, i.e. 32, 64 or 128).
 // For every "theirs" element j the CUDA cores compute the exact fixed-point
 // phase and e = (cos, sin) of the angle once per row, split each component
 // into a TF32 head and tail (v = hi + lo, hi = v rounded to TF32) and store
@@ -27,9 +29,13 @@
 //
 // Warp roles (4 H + 2 warps; H = 2):
 //   warps 0 .. 4H-1   A producers: warp w writes lanes 32 (w % 4) .. +31 for
-//                     the "theirs" share w / 4 (of H) of every chunk; groups
-//                     0 .. PT-1 also drain the accumulators of row tile
-//                     (w / 4) and write the partial sums
+//                     the "theirs" share w / 4 (of H) of every chunk and
+//                     expands its share of the chunk's B; with PT = 2 group g
+//                     drains the accumulators of row tile g, with PT = 1 group
+//                     g drains the head and tail columns of coils
+//                     [g CG / 2, (g + 1) CG / 2) (the adjoint's coil sum then
+//                     completes across the groups in shared memory); all write
+//                     the partial sums
 //   warp 4H           bulk loads of the "theirs" tiles
 //   warp 4H + 1       tensor-memory allocation and the MMA issue (lane 0)
 // Every mbarrier wait is bounded; on expiry DEV_ERR_TIMEOUT is raised and the
