@@ -107,19 +107,30 @@ __global__ void __launch_bounds__(kNT, OCC)
         }
         mbar_wait_bounded(&s_bar[b], (t >> 1) & 1, err);
 
-        // per-tile partial sums keep the FP32 accumulation error small
-        float tr[PT][CG], ti[PT][CG];
+        // per-tile partial sums keep the FP32 accumulation error small.  Rows
+        // 2m and 2m + 1 share one packed FP32x2 FMA (sm_100 FFMA2: two FMAs per
+        // instruction, each rounded as fmaf), so every element is computed
+        //     tr = fma(dx, cs, fma(dy, sn, tr)),  ti = fma(dy, cs, fma(dx, -sn, ti))
+        // in the order of the scalar form, with half the multiply-add instructions.
+        static_assert(PT % 2 == 0, "rows are packed in pairs");
+        constexpr int PP = PT / 2;
+        float2 tr[PP][CG], ti[PP][CG];
 #pragma unroll
-        for (int j = 0; j < PT; ++j)
+        for (int m = 0; m < PP; ++m)
 #pragma unroll
-            for (int c = 0; c < CG; ++c) tr[j][c] = ti[j][c] = 0.f;
+            for (int c = 0; c < CG; ++c) tr[m][c] = ti[m][c] = make_float2(0.f, 0.f);
 
 #pragma unroll 2
         for (int v = 0; v < kTile; ++v) {
             const double4 q = s_geo[b][v];
-            float2 dv[CG];
+            float2 dx2[CG], dy2[CG];  // the datum broadcast to both rows of a pair
 #pragma unroll
-            for (int c = 0; c < CG; ++c) dv[c] = s_dat[b][v * CG + c];
+            for (int c = 0; c < CG; ++c) {
+                const float2 d = s_dat[b][v * CG + c];
+                dx2[c] = make_float2(d.x, d.x);
+                dy2[c] = make_float2(d.y, d.y);
+            }
+            float cs[PT], sn[PT];
 #pragma unroll
             for (int j = 0; j < PT; ++j) {
                 double acc = fma(ox[j], q.x, kMagic);
@@ -130,21 +141,28 @@ __global__ void __launch_bounds__(kNT, OCC)
                 const float f1 = __uint_as_float(__funnelshift_r(P, 0x7Fu, 9));
                 const float ang =
                     ADJ ? fmaf(f1, -kTwoPiF, kThreePiF) : fmaf(f1, kTwoPiF, -kThreePiF);
-                float sn, cs;
-                __sincosf(ang, &sn, &cs);
+                __sincosf(ang, &sn[j], &cs[j]);
+            }
+#pragma unroll
+            for (int m = 0; m < PP; ++m) {
+                const float2 c2 = make_float2(cs[2 * m], cs[2 * m + 1]);
+                const float2 s2 = make_float2(sn[2 * m], sn[2 * m + 1]);
+                const float2 ns2 = make_float2(-sn[2 * m], -sn[2 * m + 1]);
 #pragma unroll
                 for (int c = 0; c < CG; ++c) {
-                    tr[j][c] = fmaf(dv[c].x, cs, fmaf(dv[c].y, sn, tr[j][c]));
-                    ti[j][c] = fmaf(dv[c].y, cs, fmaf(-dv[c].x, sn, ti[j][c]));
+                    tr[m][c] = __ffma2_rn(dx2[c], c2, __ffma2_rn(dy2[c], s2, tr[m][c]));
+                    ti[m][c] = __ffma2_rn(dy2[c], c2, __ffma2_rn(dx2[c], ns2, ti[m][c]));
                 }
             }
         }
 #pragma unroll
-        for (int j = 0; j < PT; ++j)
+        for (int m = 0; m < PP; ++m)
 #pragma unroll
             for (int c = 0; c < CG; ++c) {
-                ar[j][c] += tr[j][c];
-                ai[j][c] += ti[j][c];
+                ar[2 * m][c] += tr[m][c].x;
+                ar[2 * m + 1][c] += tr[m][c].y;
+                ai[2 * m][c] += ti[m][c].x;
+                ai[2 * m + 1][c] += ti[m][c].y;
             }
         __syncthreads();
     }
