@@ -12,7 +12,9 @@
 // The phase is the 4-term dot product ours.(x,y,z,w) . theirs.(x,y,z,w) in
 // turns, so one kernel template serves both directions.  Tiles of "theirs"
 // (geometry + per-coil data) are moved by cp.async.bulk onto an mbarrier,
-// double buffered.  The "theirs" range is split across blockIdx.y; each split
+// double buffered.  The per-coil complex multiply-add of two "ours" rows runs
+// as packed FP32x2 FMAs (sm_100 FFMA2), element by element the scalar fmaf
+// sequence.  The "theirs" range is split across blockIdx.y; each split
 // writes deterministic partial sums that a small kernel adds up.
 #include "nudft.cuh"
 #include "common.cuh"
