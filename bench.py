@@ -344,7 +344,7 @@ C1_METRIC = "s/recon (brute-force 2-D CG, 64x64, 1 coil, M=4096, 8 CG x 10 TV)"
 
 
 def run_bf2d(args, ws, rank, local):
-    """Configuration 1, the reference's CPU-runnable case: 2-D 64x64, one coil,
+    """The reference's CPU-runnable case: 2-D 64x64, one coil,
     4 x 1024 spiral (M = 4096), field map, TV lambda 1e-3 with 10 reweighting
     passes (the reference's -tv default) of 8 CG iterations.  Data: this
     library's exact-phase NUDFT of the seeded phantom + 40 dB noise.  The CPU
@@ -760,7 +760,7 @@ BATCH_METRIC = ("s/recon (brute-force CG, 64 independent 2-D 384x384 slices, 32 
 
 
 def run_batch(args, ws, rank, local):
-    """Configuration 4: independent 384x384 slices with 32 ring coils, each with
+    """64 independent 384x384 slices with 32 ring coils, each with
     its own seeded spiral of 16..32 interleaves x 4096 samples (uneven M), field
     map and phantom; plain CG, cg_num 20 (19 updates).  The timed job is the
     first `--slices` slices of the seeded 64; with N GPUs each rank takes a

@@ -146,7 +146,7 @@ struct TcShape {
     static constexpr int CHUNKS = kTile / KC;         // chunks per "theirs" tile
     static constexpr int ACOLS = 4 * KC;              // A columns per row tile per chunk
     // A (and B) chunk buffers (three, where tensor memory holds them, measured
-    // the same: configuration 4 98.2 s against 98.5 s)
+    // the same on the 64-slice 384x384 32-coil batch: 98.2 s against 98.5 s)
     static constexpr int NB = 2;
     static constexpr int NBB = NB;                    // B chunk buffers (paired with A's)
     static constexpr int DCOLS = 2 * PT * NN;         // two accumulator sets
