@@ -67,6 +67,18 @@ def test_noalloc_adjoint_matches_regular_twice(pkg, synth):
         assert oracle.rel_l2(a, b) < TOL_OP
 
 
+def test_noalloc_adjoint_tensor_core_coil_group(pkg, synth):
+    """Twenty coils: one coil group of 32 on the tensor-core kernel inside the
+    static array, against the regular adjoint and the FP64 oracle."""
+    c = _inputs(synth, 32, 1, 20, 2048, seed=3)
+    a = _noalloc(pkg, c)
+    b = _regular(pkg, c)
+    assert oracle.rel_l2(a, b) < TOL_OP
+    case = dict(c)
+    ref = oracle.ift(c["d"].reshape(c["C"], -1), case, use_z=0)
+    assert oracle.rel_l2(a, ref) < TOL_OP
+
+
 def test_noalloc_rejects_sizes_beyond_the_scratch(pkg, synth):
     import torch
     M, N = 1 << 20, 1 << 20
