@@ -44,6 +44,7 @@ EXPORTED = [
     "imp_bruteforce_batch", "imp_bruteforce_mgpu",
     "imp_dataset_info", "imp_mrisolver_main", "imp_measure_alu_peaks",
     "imp_toeplitz_options_default", "imp_toeplitz_q", "imp_toeplitz_fhd", "imp_toeplitz_recon",
+    "imp_grid_fft",
     "imp_toeplitz_apply", "imp_toeplitz_dir", "imp_toeplitz_cg",
     "imp_unet_create", "imp_unet_destroy", "imp_unet_num_params", "imp_unet_get_params",
     "imp_unet_set_params", "imp_unet_forward", "imp_unet_gradients", "imp_unet_train_step",
@@ -123,6 +124,7 @@ def lib() -> ctypes.CDLL:
         L.imp_toeplitz_fhd.argtypes = [vp, TO] + [vp] * 11 + [ip] * 5
         L.imp_toeplitz_recon.argtypes = [vp, TO] + [vp] * 7 + [ip] + [vp] * 3 + [ip] * 4
         L.imp_toeplitz_apply.argtypes = [vp, TO] + [vp] * 7 + [ip] + [vp] * 3 + [ip] * 4
+        L.imp_grid_fft.argtypes = [vp, vp, vp, ip, ip, ip, ip, ip]
         L.imp_toeplitz_dir.argtypes = [ctypes.c_char_p, TO, ip, ip, ip, ctypes.c_char_p, ip]
         L.imp_toeplitz_cg.argtypes = ([vp, TO] + [vp] * 7 + [ip] + [vp] * 3 + [ip] * 4
                                       + [ctypes.c_double, ip, ctypes.POINTER(ip)])
@@ -369,6 +371,13 @@ def toeplitz(idir: str, opts: ToepOptions, direct=False, gpu_id=0, reuseQ=False,
     _check(lib().imp_toeplitz_dir(os.fsencode(idir), ctypes.byref(opts), int(direct), gpu_id,
                                   int(reuseQ), os.fsencode(Qdir) if Qdir else None,
                                   int(writeQ)))
+
+
+def grid_fft(ctx, data_r, data_i, n0, n1, n2, batch=1, inverse=False):
+    """In-place unnormalised complex FFT of `batch` n0 x n1 x n2 grids (n2
+    fastest), split re/im float32 arrays (host numpy or CUDA tensors)."""
+    _check(lib().imp_grid_fft(ctx.handle, _ptr(data_r), _ptr(data_i), int(n0), int(n1), int(n2),
+                              int(batch), 1 if inverse else 0))
 
 
 def toeplitz_cg(ctx, opts: ToepOptions, x_r, x_i, fhd_r, fhd_i, q_r, q_i, t, num_k, fm,

@@ -78,7 +78,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
     newest = max(o.stat().st_mtime for o in objs)
     if not LIB.exists() or LIB.stat().st_mtime < newest:
         cmd = [str(cuda / "bin" / "nvcc"), *ARCH, "-shared", "-o", str(LIB), *map(str, objs),
-               f"-L{cuda / 'lib64'}", "-lcufft", f"-Xlinker=-rpath,{cuda / 'lib64'}",
+               f"-L{cuda / 'lib64'}", f"-Xlinker=-rpath,{cuda / 'lib64'}",
                "-lcudart_static", "-lrt", "-ldl", "-lpthread", "-ccbin", "g++"]
         if verbose:
             print(" ".join(cmd), flush=True)

@@ -14,9 +14,11 @@
 //   for the (at most two) time segments whose Hanning window covers the
 //   sample -- no CPU binning, no overflow path, no host round trips;
 // * every shift / crop / deapodisation / phase / SENSE step is an index map
-//   fused into the kernels around the FFTs; the FFTs are cuFFT C2C;
-// * the zero-padded F^H F input lives in a buffer whose padding is zeroed once,
-//   so a pass writes only the image block; all coils are batched in one FFT;
+//   fused into the kernels around the FFTs; the FFTs are this library's own
+//   (the pruned F^H F engine of toep_fft.cu for power-of-two images, the
+//   mixed-radix grid transform of grid_fft.cu for the gridding grids, Qf_l
+//   and the zero-padded chain of other sizes, all coils batched in one
+//   transform);
 // * Qf_l, sensitivities and phase factors stay resident in HBM; one CG
 //   iteration (FFT chain + FP64 CG scalars, best-iterate tracking and the
 //   tolerance stop all on the device) is captured once as a CUDA graph.
@@ -523,28 +525,21 @@ GridSpec grid_spec(const int img[3], float os, bool beta_after_rounding, float k
         cudaError_t e_ = (x);                   \
         if (e_ != cudaSuccess) return e_;       \
     } while (0)
-#define T_FFT(x)                                            \
-    do {                                                    \
-        if ((x) != CUFFT_SUCCESS) return cudaErrorUnknown;  \
-    } while (0)
 
 ToepSolver::~ToepSolver() { release(); }
 
 void ToepSolver::release() {
     if (g_iter_) cudaGraphExecDestroy(g_iter_);
     g_iter_ = nullptr;
-    for (cufftHandle *h : {&plan2_, &plan1_, &planq_, &planf_})
-        if (*h) {
-            cufftDestroy(*h);
-            *h = 0;
-        }
-    std::memset(planq_dims_, 0, sizeof(planq_dims_));
-    std::memset(planf_dims_, 0, sizeof(planf_dims_));
-    void *bufs[] = {sens_, eph_, fm_, qf_, pad_, big_, x_, r_, p_, q_, best_, fhd_, w_, dots_,
+    for (GridFft *f : {&gf2_, &gf1_, &gfq_, &gff_}) {
+        grid_fft_destroy(f);
+        *f = GridFft();
+    }
+    void *bufs[] = {sens_, eph_, fm_, qf_, big_, x_, r_, p_, q_, best_, fhd_, w_, dots_,
                     t_, grid_, qf2_, b1_, tw_};
     for (void *b : bufs)
         if (b) cudaFree(b);
-    sens_ = eph_ = qf_ = pad_ = big_ = x_ = r_ = p_ = q_ = best_ = fhd_ = grid_ = nullptr;
+    sens_ = eph_ = qf_ = big_ = x_ = r_ = p_ = q_ = best_ = fhd_ = grid_ = nullptr;
     qf2_ = b1_ = tw_ = nullptr;
     fast_ = false;
     fm_ = w_ = t_ = nullptr;
@@ -618,9 +613,9 @@ cudaError_t ToepSolver::setup(const ToepConfig &cfg, const float *t, const float
     T_TRY(cudaMalloc(&sens_, sizeof(float2) * C * N_));
     T_TRY(cudaMalloc(&eph_, sizeof(float2) * L1 * N_));
     // The pruned FFT engine needs power-of-two image sizes; other sizes (and
-    // IMP_TOEP_CUFFT=1) use the zero-padded cuFFT chain.
-    const char *force_cufft = std::getenv("IMP_TOEP_CUFFT");
-    fast_ = !(force_cufft && force_cufft[0] == '1') &&
+    // IMP_TOEP_PADDED=1) use the zero-padded chain on the grid transform.
+    const char *force_padded = std::getenv("IMP_TOEP_PADDED");
+    fast_ = !(force_padded && force_padded[0] == '1') &&
             toep_fft_plan(nv[0], is3d ? nv[1] : 1, is3d ? nv[2] : nv[1], C, &fp_);
     if (fast_) {
         T_TRY(cudaMalloc(&qf_, sizeof(float2) * G2_));  // one segment, before permutation
@@ -629,40 +624,31 @@ cudaError_t ToepSolver::setup(const ToepConfig &cfg, const float *t, const float
         T_TRY(toep_fft_twiddles(&tw_));
     } else {
         T_TRY(cudaMalloc(&qf_, sizeof(float2) * L1 * G2_));
-        T_TRY(cudaMalloc(&pad_, sizeof(float2) * C * G2_));
         T_TRY(cudaMalloc(&big_, sizeof(float2) * C * G2_));
     }
     for (float2 **b : {&x_, &r_, &p_, &q_, &best_, &fhd_}) T_TRY(cudaMalloc(b, sizeof(float2) * N_));
     T_TRY(cudaMalloc(&w_, sizeof(float) * N_));
     T_TRY(cudaMalloc(&dots_, sizeof(double) * (T_SCAL * kTBlocks + 8)));
     T_TRY(cudaMemsetAsync(dots_, 0, sizeof(double) * (T_SCAL * kTBlocks + 8), st));
-    if (!fast_) T_TRY(cudaMemsetAsync(pad_, 0, sizeof(float2) * C * G2_, st));
     k_pack_sens_c<<<gridn((size_t)C * N_), kVB, 0, st>>>(sens_, sensi_r, sensi_i, (size_t)C * N_);
     k_eph<<<gridn((size_t)L1 * N_), kVB, 0, st>>>(eph_, fm, N_, L1, tau_, t0_);
     T_TRY(cudaGetLastError());
-    // batched C2C on the 2N grid (one transform per coil) and a single one for Qf
-    int dims[3] = {n2[0], n2[1], n2[2]};
-    const int rank = is3d ? 3 : 2;
-    if (!fast_) {
-        T_FFT(cufftPlanMany(&plan2_, rank, dims, nullptr, 1, (int)G2_, nullptr, 1, (int)G2_,
-                            CUFFT_C2C, C));
-        T_FFT(cufftSetStream(plan2_, st));
-    }
-    T_FFT(cufftPlanMany(&plan1_, rank, dims, nullptr, 1, (int)G2_, nullptr, 1, (int)G2_, CUFFT_C2C,
-                        1));
-    T_FFT(cufftSetStream(plan1_, st));
+    // the 2N grid: batched over the coils for the zero-padded chain, single
+    // for Qf_l (2-D grids are [n2[0]][n2[1]], 3-D [n2[0]][n2[1]][n2[2]])
+    const int d0 = is3d ? n2[0] : 1, d1 = is3d ? n2[1] : n2[0], d2 = is3d ? n2[2] : n2[1];
+    if (!fast_) T_TRY(grid_fft_create(&gf2_, d0, d1, d2, C));
+    T_TRY(grid_fft_create(&gf1_, d0, d1, d2, 1));
     launches_ = 2;
     return cudaSuccess;
 }
 
-cudaError_t ToepSolver::ensure_grid_plan(const GridSpec &g, cufftHandle *plan, int *dc) {
-    if (*plan && dc[0] == g.gs[0] && dc[1] == g.gs[1] && dc[2] == g.gs[2]) return cudaSuccess;
-    if (*plan) cufftDestroy(*plan);
-    *plan = 0;
-    int dims[3] = {g.gs[0], g.gs[1], g.gs[2]};
-    T_FFT(cufftPlanMany(plan, g.is3d ? 3 : 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_C2C, 1));
-    T_FFT(cufftSetStream(*plan, st_));
-    for (int a = 0; a < 3; ++a) dc[a] = g.gs[a];
+cudaError_t ToepSolver::ensure_grid_plan(const GridSpec &g, GridFft *plan) {
+    const int d0 = g.is3d ? g.gs[0] : 1, d1 = g.is3d ? g.gs[1] : g.gs[0];
+    const int d2 = g.is3d ? g.gs[2] : g.gs[1];
+    if (plan->tw[0] || plan->tw[1] || plan->tw[2]) {
+        if (plan->n[0] == d0 && plan->n[1] == d1 && plan->n[2] == d2) return cudaSuccess;
+    }
+    T_TRY(grid_fft_create(plan, d0, d1, d2, 1));
     if (g.cells() > grid_cells_) {
         if (grid_) cudaFree(grid_);
         grid_ = nullptr;
@@ -677,21 +663,21 @@ cudaError_t ToepSolver::compute_q(const float *kx, const float *ky, const float 
     const bool is3d = cfg_.nz > 1;
     const int img[3] = {2 * cfg_.nx, 2 * cfg_.ny, is3d ? 2 * cfg_.nz : 1};
     const GridSpec g = grid_spec(img, cfg_.os_q, true, 2.0f);
-    T_TRY(ensure_grid_plan(g, &planq_, planq_dims_));
+    T_TRY(ensure_grid_plan(g, &gfq_));
     const NV n2d{{n2[0], n2[1], n2[2]}};
     for (int l = 0; l <= L_; ++l) {
         T_TRY(cudaMemsetAsync(grid_, 0, sizeof(float2) * g.cells(), st_));
         k_grid<<<(cfg_.M + 127) / 128, 128, 0, st_>>>(grid_, kx, ky, kz, t_, nullptr, nullptr,
                                                       cfg_.M, g, tau_, t0_, l);
         T_TRY(cudaGetLastError());
-        T_FFT(cufftExecC2C(planq_, grid_, grid_, CUFFT_INVERSE));
+        T_TRY(grid_fft_exec(gfq_, grid_, true, st_));
         float2 *qf_l = fast_ ? qf_ : qf_ + (size_t)l * G2_;
         k_q_post<<<gridn(G2_), kVB, 0, st_>>>(grid_, g, n2d, qf_l,
                                              q_out_r ? q_out_r + (size_t)l * G2_ : nullptr,
                                              q_out_i ? q_out_i + (size_t)l * G2_ : nullptr, G2_);
         T_TRY(cudaGetLastError());
-        T_FFT(cufftExecC2C(plan1_, qf_l, qf_l, CUFFT_FORWARD));
-        launches_ += 2;  // own kernels only (cuFFT launches are not counted)
+        T_TRY(grid_fft_exec(gf1_, qf_l, false, st_));
+        launches_ += 2 + gfq_.passes() + gf1_.passes();
         if (fast_) {
             T_TRY(toep_fft_qf(fp_, qf2_ + (size_t)l * G2_, qf_l, 1.0f / (float)G2_, st_));
             ++launches_;
@@ -707,8 +693,8 @@ cudaError_t ToepSolver::load_q(const float *q_r, const float *q_i) {
         k_q_shift<<<gridn(G2_), kVB, 0, st_>>>(q_r + (size_t)l * G2_, q_i + (size_t)l * G2_, n2d,
                                               cfg_.nz > 1, qf_l, G2_);
         T_TRY(cudaGetLastError());
-        T_FFT(cufftExecC2C(plan1_, qf_l, qf_l, CUFFT_FORWARD));
-        launches_ += 1;
+        T_TRY(grid_fft_exec(gf1_, qf_l, false, st_));
+        launches_ += 1 + gf1_.passes();
         if (fast_) {
             T_TRY(toep_fft_qf(fp_, qf2_ + (size_t)l * G2_, qf_l, 1.0f / (float)G2_, st_));
             ++launches_;
@@ -723,7 +709,7 @@ cudaError_t ToepSolver::compute_fhd(const float *kx, const float *ky, const floa
     const bool is3d = cfg_.nz > 1;
     const int img[3] = {cfg_.nx, cfg_.ny, cfg_.nz};
     const GridSpec g = grid_spec(img, cfg_.os_fh, false, 1.0f);
-    T_TRY(ensure_grid_plan(g, &planf_, planf_dims_));
+    T_TRY(ensure_grid_plan(g, &gff_));
     const NV nvd{{nv[0], nv[1], nv[2]}};
     (void)is3d;
     T_TRY(cudaMemsetAsync(fhd_, 0, sizeof(float2) * N_, st_));
@@ -734,11 +720,11 @@ cudaError_t ToepSolver::compute_fhd(const float *kx, const float *ky, const floa
                 grid_, kx, ky, kz, t_, kd_r + (size_t)c * cfg_.M, kd_i + (size_t)c * cfg_.M,
                 cfg_.M, g, tau_, t0_, l);
             T_TRY(cudaGetLastError());
-            T_FFT(cufftExecC2C(planf_, grid_, grid_, CUFFT_INVERSE));
+            T_TRY(grid_fft_exec(gff_, grid_, true, st_));
             k_fh_post<<<gridn(N_), kVB, 0, st_>>>(grid_, g, nvd, N_, sens_ + (size_t)c * N_,
                                                  eph_ + (size_t)l * N_, fhd_);
             T_TRY(cudaGetLastError());
-            launches_ += 2;
+            launches_ += 2 + gff_.passes();
         }
     if (fhd_r) {
         k_c2soa<<<gridn(N_), kVB, 0, st_>>>(fhd_r, fhd_i, fhd_, N_);
@@ -766,12 +752,13 @@ cudaError_t ToepSolver::apply_aha(const float2 *p, float2 *q) {
     }
     for (int l = 0; l <= L_; ++l) {
         const float2 *eph_l = eph_ + (size_t)l * N_;
-        k_pad<<<gridn(N_), kVB, 0, st_>>>(pad_, p, sens_, eph_l, nvv, is3d, N_, G2_, C, dots);
+        T_TRY(cudaMemsetAsync(big_, 0, sizeof(float2) * C * G2_, st_));
+        k_pad<<<gridn(N_), kVB, 0, st_>>>(big_, p, sens_, eph_l, nvv, is3d, N_, G2_, C, dots);
         T_TRY(cudaGetLastError());
-        T_FFT(cufftExecC2C(plan2_, pad_, big_, CUFFT_FORWARD));
+        T_TRY(grid_fft_exec(gf2_, big_, false, st_));
         k_mulq<<<gridn((size_t)C * G2_), kVB, 0, st_>>>(big_, qf_ + (size_t)l * G2_, G2_, C, dots);
         T_TRY(cudaGetLastError());
-        T_FFT(cufftExecC2C(plan2_, big_, big_, CUFFT_INVERSE));
+        T_TRY(grid_fft_exec(gf2_, big_, true, st_));
         k_crop_acc<<<gridn(N_), kVB, 0, st_>>>(q, big_, sens_, eph_l, nvv, is3d, N_, G2_, C,
                                               l == 0 ? 1 : 0, scale, dots);
         T_TRY(cudaGetLastError());
@@ -1171,6 +1158,48 @@ imp_status imp_toeplitz_cg(imp_context *ctx, const imp_toeplitz_options *opt, fl
     if (hi && (s = copy_out(ctx, x_i, dxi, N))) return s;
     s = imp::finish(ctx);
     ctx->launches = ts->launches();
+    return s;
+}
+
+imp_status imp_grid_fft(imp_context *ctx, float *data_r, float *data_i, int n0, int n1, int n2,
+                        int batch, int inverse) {
+    if (!data_r || !data_i) return fail(IMP_ERR_INVALID_ARG, "null array argument");
+    if (n0 < 1 || n1 < 1 || n2 < 1 || batch < 1)
+        return fail(IMP_ERR_INVALID_ARG, "grid sizes and batch must be >= 1");
+    const size_t n = (size_t)batch * n0 * n1 * n2;
+    if (n > ((size_t)1 << 31)) return fail(IMP_ERR_INVALID_ARG, "grid larger than 2^31 points");
+    imp_status s = imp::begin(ctx);
+    if (s != IMP_OK) return s;
+    imp::GridFft f;
+    const cudaError_t pe = imp::grid_fft_create(&f, n0, n1, n2, batch);
+    if (pe == cudaErrorInvalidValue)
+        return fail(IMP_ERR_UNSUPPORTED, "grid FFT: an axis is longer than 4096 points or has "
+                                         "a prime factor above 255");
+    IMP_CUDA(pe, "grid FFT plan");
+    std::unique_ptr<imp::GridFft, void (*)(imp::GridFft *)> guard(&f, imp::grid_fft_destroy);
+    DevKeep keep;
+    const float *dr, *di;
+    float *odr, *odi;
+    bool hr, hi;
+    if ((s = imp::to_device(ctx, data_r, n, keep, &dr, nullptr)) ||
+        (s = imp::to_device(ctx, data_i, n, keep, &di, nullptr)) ||
+        (s = imp::out_device(ctx, data_r, n, keep, &odr, &hr)) ||
+        (s = imp::out_device(ctx, data_i, n, keep, &odi, &hi)))
+        return s;
+    void *buf = nullptr;
+    IMP_CUDA(cudaMalloc(&buf, n * sizeof(float2)), "grid FFT buffer");
+    keep.emplace_back(buf, [](void *q) { cudaFree(q); });
+    float2 *b = (float2 *)buf;
+    const cudaStream_t st = ctx->stream;
+    imp::k_soa2c<<<imp::gridn(n), imp::kVB, 0, st>>>(b, dr, di, n);
+    IMP_CUDA(cudaGetLastError(), "grid FFT pack");
+    IMP_CUDA(imp::grid_fft_exec(f, b, inverse != 0, st), "grid FFT");
+    imp::k_c2soa<<<imp::gridn(n), imp::kVB, 0, st>>>(odr, odi, b, n);
+    IMP_CUDA(cudaGetLastError(), "grid FFT unpack");
+    if (hr && (s = copy_out(ctx, data_r, odr, n))) return s;
+    if (hi && (s = copy_out(ctx, data_i, odi, n))) return s;
+    s = imp::finish(ctx);
+    ctx->launches = 2 + f.passes();
     return s;
 }
 

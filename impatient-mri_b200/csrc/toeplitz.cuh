@@ -4,9 +4,9 @@
 // toeplitz/recon.cu).
 #pragma once
 #include <cuda_runtime.h>
-#include <cufft.h>
 #include <vector>
 
+#include "grid_fft.cuh"
 #include "toep_fft.cuh"
 
 namespace imp {
@@ -81,7 +81,7 @@ public:
 private:
     cudaError_t apply_aha(const float2 *p, float2 *q);  // q = A^H A p (no TV term)
     cudaError_t cg_iteration();
-    cudaError_t ensure_grid_plan(const GridSpec &g, cufftHandle *plan, int *dims_cache);
+    cudaError_t ensure_grid_plan(const GridSpec &g, GridFft *plan);
 
     ToepConfig cfg_;
     cudaStream_t st_ = nullptr;
@@ -96,22 +96,20 @@ private:
     float2 *eph_ = nullptr;    // [(L+1)][N] exp(-i fm (tau l + t0))
     float *fm_ = nullptr;      // [N]
     float2 *qf_ = nullptr;     // [(L+1)][G2] (one segment of scratch with the engine)
-    float2 *pad_ = nullptr;    // [C][G2] zero outside the image block
-    float2 *big_ = nullptr;    // [C][G2]
+    float2 *big_ = nullptr;    // [C][G2] zero-padded chain (sizes the engine does not take)
     float2 *x_ = nullptr, *r_ = nullptr, *p_ = nullptr, *q_ = nullptr, *best_ = nullptr;
     float2 *fhd_ = nullptr;
     float *w_ = nullptr;
     double *dots_ = nullptr;   // block partials + scalars
     float *t_ = nullptr;       // copy of t [M]
-    cufftHandle plan2_ = 0;    // batched C2C on the 2N grid (batch C)
-    cufftHandle plan1_ = 0;    // single C2C on the 2N grid
-    cufftHandle planq_ = 0, planf_ = 0;  // gridding grids
-    int planq_dims_[3] = {0, 0, 0}, planf_dims_[3] = {0, 0, 0};
+    GridFft gf2_;              // 2N grid, batch C (zero-padded chain)
+    GridFft gf1_;              // 2N grid, one transform (Qf_l)
+    GridFft gfq_, gff_;        // gridding grids of Q and F^H d
     float2 *grid_ = nullptr;   // gridding scratch
     size_t grid_cells_ = 0;
     cudaGraphExec_t g_iter_ = nullptr;
     long launches_ = 0;
-    // pruned FFT engine (power-of-two sizes); the cuFFT chain otherwise
+    // pruned FFT engine (power-of-two sizes); the zero-padded chain otherwise
     bool fast_ = false;
     ToepFftPlan fp_;
     float2 *qf2_ = nullptr;    // [(L+1)][G2] Qf_l in parity-major order, scaled 1/G2

@@ -105,8 +105,14 @@ class ToepProblem:
                                     self.t, self.M, self.fm, self.sr, self.si, self.C, self.n,
                                     self.n, 1, tol=tol, max_iter=max_iter)
 
+    def make_rhs(self, n_img: int, seed: int, snr_db: float = 40.0):
+        """(b [n][2][N], x_true [n][2][N]) on the GPU, without CG labels."""
+        b, _, xt = self.make_pairs(n_img, seed, snr_db, label_iters=0)
+        return b, xt
+
     def make_pairs(self, n_img: int, seed: int, snr_db: float = 40.0, label_iters: int = 50):
-        """(b [n][2][N], label [n][2][N], x_true [n][2][N]) on the GPU."""
+        """(b [n][2][N], label [n][2][N], x_true [n][2][N]) on the GPU
+        (label_iters = 0: no labels, the second entry is None)."""
         torch = _torch()
         rng = np.random.default_rng(seed)
         n, N = self.n, self.N
@@ -129,6 +135,8 @@ class ToepProblem:
             noise *= sig[i]
             self.fhd(noise, fhn)
             b[i] += fhn
+        if label_iters <= 0:
+            return b, None, xt
         lab = torch.zeros_like(xt)
         for i in range(n_img):
             self.cg(b[i], lab[i], 0.0, label_iters)
@@ -239,6 +247,38 @@ def evaluate(prob: ToepProblem, net1, kappa: float, b, target: float = 1e-3, tol
                         warm_s=t_w, warm_nrmse=nrmse(xw, ref), x0_nrmse=nrmse(xw0, ref),
                         zero_iters_tol=it_rz, warm_iters_tol=it_rw))
     return out
+
+
+def warm_start(net1, kappa: float, b, out=None):
+    """Network output for right-hand side b ([2][N]), rescaled to a CG
+    starting image (b / rms(b) in, x0 = y rms(b) kappa out)."""
+    torch = _torch()
+    s = float(rms(b.unsqueeze(0))[0])
+    y = torch.zeros(1, 2, b.shape[-1], device="cuda")
+    net1.forward((b / s).unsqueeze(0).contiguous(), y)
+    x0 = y[0] * (s * kappa)
+    if out is not None:
+        out.copy_(x0)
+        return out
+    return x0.contiguous()
+
+
+def timed_run(prob, b, x0, k, flush=None, net1=None, kappa=None):
+    """Device time (CUDA events, ms) of one solve: k CG updates from x0, or
+    -- with net1 -- the network's starting image followed by k updates.
+    `flush` (a tensor larger than L2) is overwritten before the start event."""
+    torch = _torch()
+    x = x0.clone() if net1 is None else torch.zeros_like(b)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if flush is not None:
+        flush.fill_(1.0)
+    e0.record()
+    if net1 is not None:
+        warm_start(net1, kappa, b, out=x)
+    prob.cg(b, x, 0.0, k)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), x
 
 
 def save_weights(path, params, kappa: float, meta: dict):

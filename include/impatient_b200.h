@@ -122,10 +122,13 @@ imp_status imp_parallel_ift(imp_context *ctx, float *idata_r, float *idata_i,
  *     with IMP_ERR_INVALID_ARG.  About 40 bytes per voxel and 40 bytes per
  *     sample per group of up to 8 coils are needed, plus partial sums.
  *   - Runs on `stream` (a cudaStream_t; NULL is the legacy default stream) of
- *     the current device and returns when the result is in idata.
+ *     the current device, synchronizes that stream and returns when the
+ *     result is in idata; a failing call also drains its own queued work
+ *     before it returns.  imp_last_error() describes a failure.
  *   - The first call on a device looks up the device address of the array
  *     with that device current; make that first call before any stream
- *     capture.
+ *     capture.  The address is kept for the process: do not call this after
+ *     a cudaDeviceReset.
  *   - Every call shares the array: calls that overlap on the GPU race. */
 imp_status imp_parallel_ift_noalloc(float *idata_r, float *idata_i, const float *kdata_r,
                                     const float *kdata_i, const float *kx, const float *ky,
@@ -264,6 +267,17 @@ imp_status imp_toeplitz_recon(imp_context *ctx, const imp_toeplitz_options *opt,
                               const float *q_r, const float *q_i, const float *t, int num_k,
                               const float *fm, const float *sensi_r, const float *sensi_i,
                               int num_coil, int nx, int ny, int nz);
+
+/* In-place complex FFT of `batch` grids of n0 x n1 x n2 points (row-major, n2
+ * fastest; n0 = 1 for 2-D, n0 = n1 = 1 for 1-D), split re/im, host or device
+ * pointers: forward X[k] = sum_j x[j] e^{-2 pi i jk/n} per axis (inverse != 0:
+ * e^{+...}), unnormalised.  The transform the Toeplitz path runs on its
+ * gridding grids and on the 2N grid; replaces the cuFFT C2C calls at
+ * toeplitz/recon.cu:1161,1177,1959, toeplitz/computeQ.cmem.cu:623 and
+ * toeplitz/computeFH.cmem.cu:679.  Axes up to 4096 points whose prime factors
+ * are <= 255 (IMP_ERR_UNSUPPORTED otherwise). */
+imp_status imp_grid_fft(imp_context *ctx, float *data_r, float *data_i, int n0, int n1, int n2,
+                        int batch, int inverse);
 
 /* One application of A^H A p (+ lambda D^H D p when enable_fd), the operator
  * inside each Toeplitz CG iteration (toeplitz/recon.cu:598-840 with

@@ -26,6 +26,18 @@ from __future__ import annotations
 
 import numpy as np
 
+try:  # the same FP64 pocketfft transforms as numpy's, on all host threads
+    import scipy.fft as _sfft
+
+    def _fftn(a, axes=None):
+        return _sfft.fftn(a, axes=axes, workers=-1)
+
+    def _ifftn(a, axes=None):
+        return _sfft.ifftn(a, axes=axes, workers=-1)
+except ImportError:  # pragma: no cover
+    _fftn = np.fft.fftn
+    _ifftn = np.fft.ifftn
+
 F32 = np.float32
 PI32 = F32(3.1415926535897932384626433832795029)
 KW = 4.0
@@ -150,7 +162,7 @@ def grid_to_image(grid, n_img, os, beta):
     gs = grid.shape
     ndim = 2 if n_img[2] == 1 else 3
     g = grid[:, :, 0] if ndim == 2 else grid
-    img = np.fft.fftshift(np.fft.ifftn(np.fft.ifftshift(g)) * g.size)
+    img = np.fft.fftshift(_ifftn(np.fft.ifftshift(g)) * g.size)
     sl = tuple(slice(gs[a] // 2 - n_img[a] // 2, gs[a] // 2 - n_img[a] // 2 + n_img[a])
                for a in range(ndim))
     img = img[sl]
@@ -219,7 +231,7 @@ def qf_from_q(Q):
     out = []
     for q in Q:
         g = q if q.ndim == 2 else np.transpose(q, (1, 0, 2))
-        out.append(np.fft.fftn(np.fft.ifftshift(g)))
+        out.append(_fftn(np.fft.ifftshift(g)))
     return np.stack(out)
 
 
@@ -231,8 +243,8 @@ def fhf(image, qf):
     big = np.zeros(qf.shape, np.complex128)
     sl = tuple(slice(s - s // 2, s - s // 2 + s) for s in n)
     big[sl] = img
-    f = np.fft.fftn(np.fft.ifftshift(big)) * qf
-    r = np.fft.fftshift(np.fft.ifftn(f) * f.size)[sl] / qf.size
+    f = _fftn(np.fft.ifftshift(big)) * qf
+    r = np.fft.fftshift(_ifftn(f) * f.size)[sl] / qf.size
     return r if image.ndim == 2 else np.transpose(r, (1, 0, 2))
 
 
@@ -246,6 +258,29 @@ def aha(p, Qf, sens, fm, tau, t0):
             ph = np.exp(-1j * fm * (tau * l + t0))
             acc += np.conj(ph) * fhf(s * p * ph, Qf[l])
         out += np.conj(s) * acc
+    return out
+
+
+def aha_coils(p, Qf, sens, fm, tau, t0):
+    """aha() with the coils batched into one FFT call per segment (the same
+    FP64 arithmetic, for many coils at large sizes).  p: image in voxel
+    order; sens [C, *p.shape]; Qf [L+1, *grid] in FFT axis order."""
+    tr = p.ndim == 3
+    img_t = (lambda a: np.transpose(a, (0, 2, 1, 3))) if tr else (lambda a: a)
+    sens = np.asarray(sens).reshape(len(sens), *p.shape)
+    n = p.shape if not tr else (p.shape[1], p.shape[0], p.shape[2])
+    gshape = Qf.shape[1:]
+    sl = (slice(None),) + tuple(slice(m - m // 2, m - m // 2 + m) for m in n)
+    axes = tuple(range(1, len(gshape) + 1))
+    out = np.zeros(p.shape, np.complex128)
+    for l in range(len(Qf)):
+        ph = np.exp(-1j * np.asarray(fm, np.float64).reshape(p.shape) * (tau * l + t0))
+        big = np.zeros((len(sens),) + gshape, np.complex128)
+        big[sl] = img_t(sens * (p * ph))
+        f = _fftn(np.fft.ifftshift(big, axes=axes), axes=axes)
+        f *= Qf[l]
+        r = np.fft.fftshift(_ifftn(f, axes=axes), axes=axes)[sl] * (f[0].size / Qf[l].size)
+        out += np.conj(ph) * np.sum(np.conj(sens) * img_t(r), axis=0)
     return out
 
 

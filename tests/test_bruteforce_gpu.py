@@ -49,6 +49,23 @@ def test_bf_2d_long_tv_no_worse_than_reference_fp32(pkg, ctx):
     assert err < max(2.0 * err32, TOL_IMG)
 
 
+def test_bf2d_64_timed_config_no_worse_than_reference_fp32(pkg, ctx):
+    """The 2-D one-coil configuration that bench.py times (64x64, 4 x 1024
+    spiral, field map, cg_num 8, TV lambda 1e-3 with 10 passes), on the same
+    inputs (tests/golden/bf2d_64_timed.npz): a chaotic run (10 reweighting
+    passes), so the gate is the reference's own FP32 build against its FP64
+    build, as in the long-TV test above."""
+    from gpu_util import gpu_recon
+    c = golden("bf2d_64_timed")
+    x = gpu_recon(pkg, ctx, c, cg_num=int(c["cg_num"]), lam=float(c["lam"]), tv=True,
+                  tv_num=int(c["tv_num"]), eps=1e-6)
+    err = oracle.rel_l2(x, c["x64"])
+    err32 = oracle.rel_l2(c["x32"], c["x64"])
+    print(f"timed 2-D configuration: GPU vs reference FP64 {err:.2e}; reference FP32 vs "
+          f"FP64 {err32:.2e}")
+    assert err < max(2.0 * err32, TOL_IMG)
+
+
 def test_bf_2d_sense_matches_reference_fp64(pkg, ctx):
     from gpu_util import gpu_recon
     c = golden("bf_2d_c3")

@@ -192,6 +192,32 @@ def test_apply_sizes_match_oracle(pkg, ctx, dims, C, L):
 
 
 @pytest.mark.parametrize("dims", [(256, 256, 32), (512, 512, 1)])
+def test_apply_production_sizes_match_oracle(pkg, ctx, dims):
+    """One A^H A (+ lambda D^H D) application at the sizes the benchmarks run:
+    the 3-D 256x256x32 image (two-pass n = 256 line transforms, s = 256 on the
+    slow axis) and the 2-D 512x512 image (two-pass n = 512), both on the
+    plane kernels instantiated on compile-time geometry, against the FP64
+    oracle with random Q, field map and sensitivities (2 coils, 2 segments)."""
+    rng = np.random.default_rng(sum(dims) + 101)
+    nx, ny, nz = dims
+    C, L, M = 2, 1, 64
+    N, G = nx * ny * nz, grid_elems(dims)
+    c = dict(dims=dims, L=L, cg=1, fdp=1e-2, tv_num=0, os_q=2.0, os_fh=1.5,
+             t=np.sort(rng.uniform(0.0, 0.01, M)).astype(np.float32),
+             kx=np.zeros(M, np.float32),
+             fm=rng.uniform(-300.0, 300.0, N).astype(np.float32),
+             sens=(rng.standard_normal((C, N)) + 1j * rng.standard_normal((C, N))).astype(
+                 np.complex64))
+    Q = (rng.standard_normal((L + 1, G)) + 1j * rng.standard_normal((L + 1, G))).astype(
+        np.complex64)
+    p = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    got = gpu_apply(pkg, ctx, opts_of(pkg, c), c, Q, p)
+    err = rel(got, oracle_apply(c, Q, p, c["fdp"]))
+    print(f"apply {dims} C={C} L={L}: {err:.2e} vs the FP64 oracle")
+    assert err < TOL_OP
+
+
+@pytest.mark.parametrize("dims", [(256, 256, 32), (512, 512, 1)])
 def test_specialised_plane_kernels_match_generic(pkg, monkeypatch, dims):
     """The plane kernels instantiated on compile-time geometry (3-D 256x256x32
     and 2-D 512x512 images) give the A^H A application of the generic
