@@ -127,8 +127,13 @@ __device__ __forceinline__ void dft(float2 (&v)[R], const float2 *__restrict__) 
 // A set of 2^nl_lg lines in shared memory: line l starts at
 // (l >> lpb_lg) * bstride + (l & (2^lpb_lg - 1)) * lstride; element e of a
 // line is at start + e * es.
+// sk = 1: the line is stored skewed, r2 groups of r1 elements each followed by
+// one pad element (element x at x + x / r1), so that reading the forward
+// transform's permuted slots in natural frequency order (slot stride r1)
+// does not put a half-warp on one shared-memory bank.
 struct Lines {
     int nl_lg, lpb_lg, lstride, bstride, es;
+    int sk = 0;
 };
 
 __device__ __forceinline__ int line_base(const Lines &L, int l) {
@@ -144,7 +149,7 @@ __device__ __forceinline__ void pass_stride(float2 *buf, const Lines L, int r1, 
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
         const int l = it & ((1 << L.nl_lg) - 1), j1 = it >> L.nl_lg;
         float2 *b = buf + line_base(L, l) + j1 * L.es;
-        const int st = r1 * L.es;
+        const int st = (r1 + L.sk) * L.es;
         float2 v[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = b[q * st];
@@ -166,7 +171,7 @@ __device__ __forceinline__ void pass_contig(float2 *buf, const Lines L, int r2, 
     const int items = r2 << L.nl_lg;
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
         const int l = it & ((1 << L.nl_lg) - 1), k2 = it >> L.nl_lg;
-        float2 *b = buf + line_base(L, l) + R * k2 * L.es;
+        float2 *b = buf + line_base(L, l) + (R + L.sk) * k2 * L.es;
         float2 v[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) v[q] = b[q * L.es];
@@ -210,6 +215,7 @@ struct PlaneGeo {
     int ns, nm, nf, qm, ps, rs, ncol, C;
     int r1m, r2m, r1f, r2f;
     int lnm, lnf, lplane, lr2m, lr2f, lps;  // log2 of nm, nf, nm*nf, r2m, r2f, ps
+    int sk;                                 // rows along f stored skewed (2-D, nf > 32)
 };
 
 // The same geometry with the plane sizes as compile-time constants (the slow
@@ -217,10 +223,12 @@ struct PlaneGeo {
 // fold their per-element index arithmetic into immediates.
 template <int NM, int NF, int PS>
 struct PlaneGeoC {
-    static constexpr int nm = NM, nf = NF, ps = PS, qm = NM > 1 ? 2 : 1, rs = NF + 1;
-    static constexpr int ncol = qm * 2 * NM * NF;
     static constexpr int r1m = split_r1(NM), r2m = NM / r1m;
     static constexpr int r1f = split_r1(NF), r2f = NF / r1f;
+    static constexpr int sk = (NM == 1 && r1f > 1) ? 1 : 0;
+    static constexpr int nm = NM, nf = NF, ps = PS, qm = NM > 1 ? 2 : 1;
+    static constexpr int rs = NF + sk * r2f + 1;
+    static constexpr int ncol = qm * 2 * NM * NF;
     static constexpr int lnm = ilog2c(NM), lnf = ilog2c(NF), lplane = lnm + lnf;
     static constexpr int lr2m = ilog2c(r2m), lr2f = ilog2c(r2f), lps = ilog2c(PS);
     int ns, C;
@@ -232,6 +240,12 @@ struct PlaneGeoC {
 template <class Geo>
 constexpr bool kSmemTw = !std::is_same<Geo, PlaneGeo>::value;
 constexpr size_t kTwBytes = kTwN * sizeof(float2);
+
+// Shared-memory offset of element x of a row along f (skewed rows: x + x / r1f).
+template <class Geo>
+__device__ __forceinline__ int fphys(const Geo &g, int x) {
+    return g.sk ? x + (x >> (g.lnf - g.lr2f)) : x;
+}
 
 // Bounded mbarrier wait (about 2^22 polls); false when it ran out.
 __device__ __forceinline__ bool wait_bounded(uint64_t *bar, unsigned parity) {
@@ -266,7 +280,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fwd_plane(
     const int pstride = g.nm * g.rs;
     float2 *P = smem;
     float2 *U = smem + (size_t)g.ps * pstride;
-    const Lines rows{g.lps + g.lnm, g.lps + g.lnm, g.rs, 0, 1};
+    const Lines rows{g.lps + g.lnm, g.lps + g.lnm, g.rs, 0, 1, g.sk};
     const Lines cols{g.lps + g.lnf, g.lnf, 1, pstride, g.rs};
     const float2 *sc = sens + (size_t)c * N + vbase;
     const float2 *ec = eph_l + vbase;
@@ -288,7 +302,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fwd_plane(
                     float2 val = U[e];
                     if (am) val = cmul(val, wn(tw, m, g.lnm + 1, false));
                     if (af) val = cmul(val, wn(tw, f, g.lnf + 1, false));
-                    P[pp * pstride + m * g.rs + f] = val;
+                    P[pp * pstride + m * g.rs + fphys(g, f)] = val;
                 }
             }
             __syncthreads();
@@ -315,7 +329,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fwd_plane(
                     const int km = r >> g.lnf, kf = r & (g.nf - 1);
                     const int sm = g.nm > 1 ? slot_of(km, g.r1m, g.lr2m) : 0;
                     dst[(size_t)pp * g.ncol + r] =
-                        P[pp * pstride + sm * g.rs + slot_of(kf, g.r1f, g.lr2f)];
+                        P[pp * pstride + sm * g.rs + fphys(g, slot_of(kf, g.r1f, g.lr2f))];
                 }
             }
         }
@@ -361,7 +375,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
     if (!skip) {
         const size_t N = (size_t)g.ns << g.lplane;
         const size_t vbase = (size_t)s0 << g.lplane;
-        const Lines rows{g.lps + g.lnm, g.lps + g.lnm, g.rs, 0, 1};
+        const Lines rows{g.lps + g.lnm, g.lps + g.lnm, g.rs, 0, 1, g.sk};
         const Lines cols{g.lps + g.lnf, g.lnf, 1, pstride, g.rs};
         const int nquad = g.qm * 2;
         const int my_coils = (g.C - rank + csize - 1) / csize;
@@ -404,7 +418,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
                     const int pp = e >> g.lplane, r = e & (plane - 1);
                     const int km = r >> g.lnf, kf = r & (g.nf - 1);
                     const int sm = g.nm > 1 ? slot_of(km, g.r1m, g.lr2m) : 0;
-                    P[pp * pstride + sm * g.rs + slot_of(kf, g.r1f, g.lr2f)] = St[e];
+                    P[pp * pstride + sm * g.rs + fphys(g, slot_of(kf, g.r1f, g.lr2f))] = St[e];
                 }
             }
             __syncthreads();
@@ -433,7 +447,7 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
                 if (e < ecta) {
                     const int pp = e >> g.lplane, r = e & (plane - 1);
                     const int m = r >> g.lnf, f = r & (g.nf - 1);
-                    float2 val = P[pp * pstride + m * g.rs + f];
+                    float2 val = P[pp * pstride + m * g.rs + fphys(g, f)];
                     if (am) val = cmul(val, wn(tw, m, g.lnm + 1, true));
                     if (af) val = cmul(val, wn(tw, f, g.lnf + 1, true));
                     Y[e] = cadd(Y[e], cmulc(__ldg(&sc[e]), val));
@@ -631,6 +645,7 @@ PlaneGeo geo_of(const ToepFftPlan &p) {
     g.lr2m = ilog2c(g.r2m);
     g.lr2f = ilog2c(g.r2f);
     g.lps = ilog2c(p.ps);
+    g.sk = p.sk;
     return g;
 }
 
@@ -648,7 +663,8 @@ bool toep_fft_plan(int ns, int nm, int nf, int C, ToepFftPlan *plan) {
     p.C = C;
     const int plane = nm * nf;
     p.ps = std::max(1, std::min(ns, 8192 / plane));
-    p.rs = nf + 1;
+    p.sk = (nm == 1 && split_r1(nf) > 1) ? 1 : 0;
+    p.rs = nf + p.sk * (nf / split_r1(nf)) + 1;
     const int ecta = p.ps * plane;
     p.vpt = std::max(1, ecta / kPlaneThreads);
     p.ncol = p.qm * 2 * plane;
@@ -751,7 +767,8 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
 #undef IMP_PLANE_CASE
     const int r1 = split_r1(p.ns);
     const int cols = p.ncol / p.W;
-    const dim3 blocks(cols, std::max(1, std::min(p.C, (2 * 148 + cols - 1) / cols)));
+    // one block row per coil: enough blocks to fill every SM several times over
+    const dim3 blocks(cols, p.C);
     const int threads = p.W * r1;
 #define IMP_SLOW_CASE(NSV)                                                                 \
     case NSV:                                                                              \

@@ -28,7 +28,8 @@ struct ToepFftPlan {
     int qm = 1;                  // m parities (2 in 3-D, 1 in 2-D)
     int C = 1;                   // coils
     int ps = 1;                  // s-planes per plane-kernel block
-    int rs = 0;                  // padded shared-memory row stride (nf + 1)
+    int sk = 0;                  // 2-D rows of nf > 32 stored skewed (one pad per r1 slots)
+    int rs = 0;                  // padded shared-memory row stride (nf + sk nf / r1 + 1)
     int vpt = 1;                 // image elements per thread in the plane kernels
     int ncol = 0;                // spectrum columns per s: qm * 2 * nm * nf
     int W = 1;                   // columns per k_slow block
