@@ -57,12 +57,34 @@ class ImpError(RuntimeError):
         self.status = status
 
 
+class Sparse(ctypes.Structure):
+    """imp_sparse: a real COO matrix (0-based) in host memory; keeps its arrays."""
+    _fields_ = [
+        ("rows", ctypes.c_int), ("cols", ctypes.c_int), ("nnz", ctypes.c_int),
+        ("row", ctypes.POINTER(ctypes.c_int)), ("col", ctypes.POINTER(ctypes.c_int)),
+        ("val", ctypes.POINTER(ctypes.c_float)),
+    ]
+
+    @classmethod
+    def from_coo(cls, rows, cols, I, J, V):
+        I = np.ascontiguousarray(I, np.int32)
+        J = np.ascontiguousarray(J, np.int32)
+        V = np.ascontiguousarray(V, np.float32)
+        m = cls(int(rows), int(cols), int(I.size),
+                I.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                J.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                V.ctypes.data_as(ctypes.POINTER(ctypes.c_float)))
+        m._keep = (I, J, V)
+        return m
+
+
 class BfOptions(ctypes.Structure):
     _fields_ = [
         ("cg_num", ctypes.c_int), ("enable_fd", ctypes.c_int),
         ("fd_penalizer", ctypes.c_float), ("enable_tv", ctypes.c_int),
         ("tv_num", ctypes.c_int), ("tv_eps", ctypes.c_float), ("use_z", ctypes.c_int),
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("reg", ctypes.POINTER(Sparse)),
     ]
 
 
@@ -72,6 +94,7 @@ class ToepOptions(ctypes.Structure):
         ("fd_penalizer", ctypes.c_float), ("enable_tv", ctypes.c_int),
         ("tv_num", ctypes.c_int), ("tv_eps", ctypes.c_float), ("ntime_segs", ctypes.c_float),
         ("gridOS_Q", ctypes.c_float), ("gridOS_FH", ctypes.c_float),
+        ("reg", ctypes.POINTER(Sparse)),
     ]
 
 
@@ -243,9 +266,11 @@ def parallelIftGpu(ctx, idata_r, idata_i, kdata_r, kdata_i, kx, ky, kz, ix, iy, 
 
 
 def bf_options(cg_num=8, fd_penalizer=None, tv=False, tv_num=10, tv_eps=1e-6, use_z=0,
-               dims=None) -> BfOptions:
+               dims=None, reg=None) -> BfOptions:
     """Options of the brute-force recon; fd_penalizer enables the FD term
-    (as -fdp does, main.cpp:306-316).  dims = (nx, ny, nz) sets the TV grid."""
+    (as -fdp does, main.cpp:306-316).  dims = (nx, ny, nz) sets the TV grid.
+    reg: a Sparse roughness matrix C (-reg): lambda C^T W C replaces the FD
+    term, lambda = fd_penalizer (0 when None, as the reference's default)."""
     o = BfOptions()
     lib().imp_bf_options_default(ctypes.byref(o))
     o.cg_num = cg_num
@@ -257,6 +282,9 @@ def bf_options(cg_num=8, fd_penalizer=None, tv=False, tv_num=10, tv_eps=1e-6, us
     o.use_z = int(use_z)
     if dims is not None:
         o.nx, o.ny, o.nz = (int(d) for d in dims)
+    if reg is not None:
+        o.reg = ctypes.pointer(reg)
+        o._keep_reg = reg
     return o
 
 
@@ -320,8 +348,9 @@ def measure_alu_peaks(device: int = 0):
 
 
 def toeplitz_options(cg_num=8, fd_penalizer=None, tv=False, tv_num=10, tv_eps=1e-6,
-                     ntime_segs=12.0, gridOS_Q=1.125, gridOS_FH=1.5) -> ToepOptions:
-    """Options of the Toeplitz recon; fd_penalizer enables the FD term."""
+                     ntime_segs=12.0, gridOS_Q=1.125, gridOS_FH=1.5, reg=None) -> ToepOptions:
+    """Options of the Toeplitz recon; fd_penalizer enables the FD term, reg
+    (a Sparse roughness matrix, -reg) replaces it by lambda C^T W C."""
     o = ToepOptions()
     lib().imp_toeplitz_options_default(ctypes.byref(o))
     o.cg_num = cg_num
@@ -333,6 +362,9 @@ def toeplitz_options(cg_num=8, fd_penalizer=None, tv=False, tv_num=10, tv_eps=1e
     o.ntime_segs = float(ntime_segs)
     o.gridOS_Q = float(gridOS_Q)
     o.gridOS_FH = float(gridOS_FH)
+    if reg is not None:
+        o.reg = ctypes.pointer(reg)
+        o._keep_reg = reg
     return o
 
 

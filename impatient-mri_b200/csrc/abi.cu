@@ -404,6 +404,12 @@ static imp_status bf_config(const imp_bf_options *opt, int num_k, int num_i, int
     cfg->tv = opt->enable_tv != 0;
     cfg->tv_num = opt->enable_tv ? opt->tv_num : 1;
     cfg->tv_eps = opt->tv_eps;
+    cfg->reg = nullptr;
+    if (opt->reg) {
+        const char *why = imp::sparse_reg_check(*opt->reg, num_i);
+        if (why[0]) return fail(IMP_ERR_INVALID_ARG, std::string("-reg matrix: ") + why);
+        cfg->reg = opt->reg;
+    }
     if (opt->nx == 0 && opt->ny == 0 && opt->nz == 0) {
         // the reference's 2-D TV grid of side sqrt(N) (bruteForceGpu.cu:446-451)
         const int side = (int)std::lround(std::sqrt((double)num_i));
@@ -554,6 +560,10 @@ imp_status imp_bruteforce_batch(imp_context *ctx, const imp_bf_options *opt, flo
     // all slices in lockstep: every CG step is one launch over all slices
     imp::BfConfig cfg;
     if ((s = bf_config(opt, k_off[1] - k_off[0], num_i, num_coil, &cfg)) != IMP_OK) return s;
+    if (cfg.reg)
+        return fail(IMP_ERR_UNSUPPORTED, "-reg is not available in the batched multi-slice "
+                                         "solver; reconstruct the slices with "
+                                         "imp_bruteforce_recon");
     if (!ctx->bb) ctx->bb.reset(new imp::BfBatch());
     IMP_CUDA(ctx->bb->setup(cfg, num_slices, k_off, d_kx, d_ky, d_kz, d_t, d_ix, d_iy, d_iz, d_fm,
                             d_sr, d_si, ctx->dev_err, ctx->stream),

@@ -100,10 +100,16 @@ __global__ void k_bf_init(float2 *af, float2 *rpk, const float2 *y, const float2
     }
 }
 
-// g = sum adjoint partials - lambda D^H W D x ; partial <g,g>
+// Penalty term of the gradient and of the step length: 0 none, 1 the
+// finite-difference stencil lambda D^H W D, 2 the sparse roughness matrix
+// lambda C^T W C (with y = W C v formed beforehand).
+enum { PEN_NONE = 0, PEN_FD = 1, PEN_REG = 2 };
+
+// g = sum adjoint partials - lambda (D^H W D | C^T W C) x ; partial <g,g>
 __global__ void __launch_bounds__(kVB) k_bf_grad(float2 *g, const float2 *pa, int SG, int N,
                                                  int Npad, const float2 *x, const float *w,
-                                                 Grid3 gd, int fd, float lambda, double *dots) {
+                                                 Grid3 gd, int pen, float lambda, RegView reg,
+                                                 double *dots) {
     __shared__ double sh[33];
     double loc = 0.0;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < Npad; r += gridDim.x * blockDim.x) {
@@ -114,8 +120,8 @@ __global__ void __launch_bounds__(kVB) k_bf_grad(float2 *g, const float2 *pa, in
                 v.x += u.x;
                 v.y += u.y;
             }
-            if (fd) {
-                const float2 t = dhwd_at(x, w, r, gd);
+            if (pen) {
+                const float2 t = pen == PEN_REG ? reg_ct_at(reg, r) : dhwd_at(x, w, r, gd);
                 v.x -= lambda * t.x;
                 v.y -= lambda * t.y;
             }
@@ -173,13 +179,14 @@ __global__ void __launch_bounds__(kVB) k_bf_q(float2 *q, const float2 *pf, int S
     if (threadIdx.x == 0) dots[DOT_QQ * kDotBlocks + blockIdx.x] = b;
 }
 
-// partial Re<lambda D^H W D d, d>
+// partial Re<lambda (D^H W D | C^T W C) d, d>
 __global__ void __launch_bounds__(kVB) k_bf_tvdot(const float2 *d, const float *w, int N,
-                                                  Grid3 gd, float lambda, double *dots) {
+                                                  Grid3 gd, int pen, float lambda, RegView reg,
+                                                  double *dots) {
     __shared__ double sh[33];
     double loc = 0.0;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
-        const float2 t = dhwd_at(d, w, r, gd);
+        const float2 t = pen == PEN_REG ? reg_ct_at(reg, r) : dhwd_at(d, w, r, gd);
         const float2 dv = d[r];
         loc += (double)(lambda * t.x) * dv.x + (double)(lambda * t.y) * dv.y;
     }
@@ -273,6 +280,7 @@ void BfSolver::release() {
     if (g_iter_) cudaGraphExecDestroy(g_iter_);
     if (g_init_) cudaGraphExecDestroy(g_init_);
     g_iter_ = g_init_ = nullptr;
+    reg_.release();
     void *bufs[] = {y_, af_, q_, rpk_, xs_, x_, g_, d_, w_, pf_, pa_, dots_};
     for (void *b : bufs)
         if (b) cudaFree(b);
@@ -293,12 +301,15 @@ cudaError_t BfSolver::setup(const BfConfig &cfg, const float *kx, const float *k
                             cfg.autotune == cfg_.autotune;
     if (same_shape) {
         // keep buffers, tuned launch shapes and (if the captured scalars match) the graphs
-        if (cfg.fd != cfg_.fd || cfg.lambda != cfg_.lambda) {
+        bool stale = cfg.fd != cfg_.fd || cfg.lambda != cfg_.lambda;
+        cfg_ = cfg;
+        bool moved = false;
+        IMP_TRY(set_reg(&moved));
+        if (stale || moved) {
             if (g_iter_) cudaGraphExecDestroy(g_iter_);
             if (g_init_) cudaGraphExecDestroy(g_init_);
             g_iter_ = g_init_ = nullptr;
         }
-        cfg_ = cfg;
         return nu_plan_repack(plan_, kx, ky, kz, t, ix, iy, iz, sensi_r, sensi_i, dev_err, st);
     }
     release();
@@ -336,7 +347,27 @@ cudaError_t BfSolver::setup(const BfConfig &cfg, const float *kx, const float *k
     }
     IMP_TRY(dalloc(&dots_, (size_t)5 * kDotBlocks));
     IMP_TRY(cudaMemsetAsync(dots_, 0, sizeof(double) * 5 * kDotBlocks, st_));
+    bool moved = false;
+    IMP_TRY(set_reg(&moved));
     return cudaGetLastError();
+}
+
+// Uploads (or drops) the -reg matrix of cfg_; *graphs_stale when the penalty
+// kernels' arguments changed (matrix switched on or off, or its buffers moved).
+cudaError_t BfSolver::set_reg(bool *graphs_stale) {
+    *graphs_stale = false;
+    if (!cfg_.reg) {
+        if (reg_.on()) {
+            reg_.release();
+            *graphs_stale = true;
+        }
+        return cudaSuccess;
+    }
+    const bool was_on = reg_.on();
+    bool moved = false;
+    IMP_TRY(reg_.set(*cfg_.reg, cfg_.N, st_, &moved));
+    *graphs_stale = moved || !was_on;
+    return cudaSuccess;
 }
 
 cudaError_t BfSolver::run_init() {
@@ -361,8 +392,15 @@ cudaError_t BfSolver::run_iteration() {
     IMP_TRY(prof_mark(1));
     IMP_TRY(nu_adjoint_partials(plan_, plan_.adj, rpk_, pa_, err_, st_));
     IMP_TRY(prof_mark(1));
+    // -reg takes precedence over -fd (bruteForce/bruteForceCpu.cpp:306-325)
+    const int pen = reg_.on() ? PEN_REG : cfg_.fd ? PEN_FD : PEN_NONE;
+    int n = 5;
+    if (pen == PEN_REG) {  // y = W C x
+        IMP_TRY(reg_.apply_cw(x_, w_, nullptr, st_));
+        ++n;
+    }
     k_bf_grad<<<kDotBlocks, kVB, 0, st_>>>(g_, pa_, plan_.adj.split * plan_.G, plan_.N,
-                                           plan_.Npad, x_, w_, gd, cfg_.fd ? 1 : 0, cfg_.lambda,
+                                           plan_.Npad, x_, w_, gd, pen, cfg_.lambda, reg_.view(),
                                            dots_);
     IMP_TRY(cudaGetLastError());
     k_bf_dir<<<kDotBlocks, kVB, 0, st_>>>(d_, xs_, g_, plan_.sens, plan_.Npad, plan_.CG, plan_.G,
@@ -373,9 +411,13 @@ cudaError_t BfSolver::run_iteration() {
     IMP_TRY(prof_mark(0));
     k_bf_q<<<kDotBlocks, kVB, 0, st_>>>(q_, pf_, plan_.fwd.split, L, dots_);
     IMP_TRY(cudaGetLastError());
-    int n = 5;
-    if (cfg_.fd) {
-        k_bf_tvdot<<<kDotBlocks, kVB, 0, st_>>>(d_, w_, plan_.N, gd, cfg_.lambda, dots_);
+    if (pen == PEN_REG) {  // y = W C d
+        IMP_TRY(reg_.apply_cw(d_, w_, nullptr, st_));
+        ++n;
+    }
+    if (pen) {
+        k_bf_tvdot<<<kDotBlocks, kVB, 0, st_>>>(d_, w_, plan_.N, gd, pen, cfg_.lambda,
+                                                reg_.view(), dots_);
         IMP_TRY(cudaGetLastError());
         ++n;
     }
@@ -418,7 +460,7 @@ cudaError_t BfSolver::solve(const float *fm, const float *kd_r, const float *kd_
     for (int tv_i = 0; tv_i < std::max(cfg_.tv_num, 1); ++tv_i) {
         if (tv_i == 0)
             k_fill<<<kDotBlocks, kVB, 0, st_>>>(w_, 1.f, Npad);
-        else if (cfg_.fd)
+        else if (cfg_.fd || reg_.on())
             k_tv_weight<<<kDotBlocks, kVB, 0, st_>>>(w_, x_, N, gd, cfg_.tv_eps);
         IMP_TRY(cudaGetLastError());
         ++launches_;

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <vector>
 #include "nudft.cuh"
+#include "sparse_reg.cuh"
 
 namespace imp {
 
@@ -18,6 +19,7 @@ struct BfConfig {
     float tv_eps = 1e-6f;        // MRI_SMOOTH_FACTOR (FP32 build)
     bool use_graphs = true;
     bool autotune = true;        // time launch shapes once per problem shape
+    const imp_sparse *reg = nullptr;  // -reg roughness matrix (host COO), null = off
 };
 
 class BfSolver {
@@ -59,8 +61,11 @@ private:
     std::vector<int> prof_kind_;
     size_t prof_used_ = 0;
 
+    cudaError_t set_reg(bool *graphs_stale);
+
     BfConfig cfg_;
     NuPlan plan_;
+    SparseReg reg_;           // -reg: C and C^T on the device
     cudaStream_t st_ = nullptr;
     unsigned *err_ = nullptr;
     float2 *y_ = nullptr, *af_ = nullptr, *q_ = nullptr, *rpk_ = nullptr, *xs_ = nullptr;

@@ -35,7 +35,8 @@ void usage(FILE *f) {
                  "  -gpu_id <id>           CUDA device (default 0)\n"
                  "  -bf3d                  brute force with the true 3-D phase and 3-D TV\n"
                  "  -mgpu                  slices spread over every visible GPU (brute force)\n"
-                 "  -cpu, -nogpu, -reg     not provided by this build\n");
+                 "  -reg                   roughness regularization with the sparse matrix idir/c.rmtx\n"
+                 "  -cpu, -nogpu           not provided by this build\n");
 }
 
 }  // namespace
@@ -191,7 +192,8 @@ extern "C" imp_status imp_toeplitz_dir_cli(const char *idir, const char *odir, i
                                            int enable_fd, float fdp, int enable_tv, int tv_num,
                                            int direct, float gridOS_Q, float gridOS_FH,
                                            float ntime_segs, int gpu_id, int reuseQ,
-                                           const char *Qpath, int writeQ);
+                                           const char *Qpath, int writeQ,
+                                           const imp_sparse *reg);
 
 extern "C" int imp_mrisolver_main(int argc, char **argv) {
     std::string idir, odir;
@@ -322,9 +324,25 @@ extern "C" int imp_mrisolver_main(int argc, char **argv) {
         std::fprintf(stderr, "\n Error: Regularization enabled, but no weight parameter specified. Hint: -fdp [lambda].\n");
         return 1;
     }
+    // -reg: the roughness matrix C from idir/c.rmtx (kernels/structures.cpp:722-735);
+    // it takes precedence over -fd, which the reference only warns about
+    // (main.cpp:374-381)
+    imp::SparseCoo rc;
+    imp_sparse rs{};
     if (reg) {
-        std::fprintf(stderr, "\nError: -reg (sparse-matrix regularization) is not provided by this build.\n");
-        return 1;
+        if (fd) std::printf("mriSolver: Error: Roughness regularization and finite difference are exclusive.\n");
+        std::printf("mriSolver: Enable roughness regularization.\n");
+        std::string err;
+        if (imp::read_mtx(idir + "/c.rmtx", rc, err) != IMP_OK) {
+            std::fprintf(stderr, "\nError: %s\n", err.c_str());
+            return 1;
+        }
+        rs.rows = rc.rows;
+        rs.cols = rc.cols;
+        rs.nnz = (int)rc.val.size();
+        rs.row = rc.row.data();
+        rs.col = rc.col.data();
+        rs.val = rc.val.data();
     }
     if (nogpu || cpu) {
         std::fprintf(stderr, "\nError: -cpu / -nogpu: this build has no CPU reconstruction path.\n");
@@ -337,7 +355,7 @@ extern "C" int imp_mrisolver_main(int argc, char **argv) {
     if (tgrid || tdirect) {
         st = imp_toeplitz_dir_cli(idir.c_str(), odir.c_str(), cg_num, fd, fdp, tv, tv_num,
                                   tdirect ? 1 : 0, osQ, osFH, ntime, gpu_id, reuseQ ? 1 : 0,
-                                  Qloc.c_str(), writeQ ? 1 : 0);
+                                  Qloc.c_str(), writeQ ? 1 : 0, reg ? &rs : nullptr);
     } else {
         imp_bf_options o;
         imp_bf_options_default(&o);
@@ -347,6 +365,7 @@ extern "C" int imp_mrisolver_main(int argc, char **argv) {
         o.enable_tv = tv;
         o.tv_num = tv_num;
         o.use_z = bf3d;
+        o.reg = reg ? &rs : nullptr;
         st = imp_bruteforce_dir(idir.c_str(), odir.c_str(), &o, mgpu ? -1 : gpu_id);
     }
     if (st != IMP_OK) {

@@ -16,6 +16,7 @@
 
 #include <cerrno>
 #include <cmath>
+#include <cctype>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -165,6 +166,72 @@ int read_data_file(const std::string &fn, bool v02, DataFile &out, std::string &
     }
     out = DataFile();
     return v02 ? read_v02(fp.f, fn, out, err) : read_v10(fp.f, fn, out, err);
+}
+
+int read_mtx(const std::string &fn, SparseCoo &out, std::string &err) {
+    out = SparseCoo();
+    File fp(fn, "r");
+    if (!fp.f) {
+        err = fn + " not found";
+        return IMP_ERR_IO;
+    }
+    char line[1024];
+    if (!std::fgets(line, sizeof line, fp.f)) {
+        err = fn + ": empty file";
+        return IMP_ERR_FORMAT;
+    }
+    std::string banner(line);
+    for (char &ch : banner) ch = (char)std::tolower((unsigned char)ch);
+    if (banner.rfind("%%matrixmarket", 0) != 0) {
+        err = fn + ": could not process Matrix Market banner";
+        return IMP_ERR_FORMAT;
+    }
+    if (banner.find("coordinate") == std::string::npos || banner.find("matrix") == std::string::npos) {
+        err = fn + ": only coordinate (sparse) matrices are supported";
+        return IMP_ERR_FORMAT;
+    }
+    if (banner.find("complex") != std::string::npos) {
+        err = fn + ": complex matrices are not supported";
+        return IMP_ERR_FORMAT;
+    }
+    const bool pattern = banner.find("pattern") != std::string::npos;
+    long rows = -1, cols = -1, nnz = -1;
+    while (std::fgets(line, sizeof line, fp.f)) {
+        if (line[0] == '%') continue;
+        if (std::sscanf(line, "%ld %ld %ld", &rows, &cols, &nnz) == 3) break;
+        bool blank = true;
+        for (const char *c = line; *c; ++c)
+            if (!std::isspace((unsigned char)*c)) blank = false;
+        if (!blank) break;
+    }
+    if (rows <= 0 || cols <= 0 || nnz < 0 || rows > (1L << 30) || cols > (1L << 30) ||
+        nnz > (1L << 30)) {
+        err = fn + ": bad size line";
+        return IMP_ERR_FORMAT;
+    }
+    out.rows = (int)rows;
+    out.cols = (int)cols;
+    out.row.resize(nnz);
+    out.col.resize(nnz);
+    out.val.resize(nnz);
+    for (long e = 0; e < nnz; ++e) {
+        long i = 0, j = 0;
+        double v = 1.0;
+        const int got = pattern ? std::fscanf(fp.f, "%ld %ld", &i, &j)
+                                : std::fscanf(fp.f, "%ld %ld %lg", &i, &j, &v);
+        if (got != (pattern ? 2 : 3)) {
+            err = fn + ": failed to read entry " + std::to_string(e + 1);
+            return IMP_ERR_FORMAT;
+        }
+        if (i < 1 || i > rows || j < 1 || j > cols) {
+            err = fn + ": index out of range at entry " + std::to_string(e + 1);
+            return IMP_ERR_FORMAT;
+        }
+        out.row[e] = (int)(i - 1);
+        out.col[e] = (int)(j - 1);
+        out.val[e] = (float)v;
+    }
+    return IMP_OK;
 }
 
 int load_input_dir(const std::string &dir, Dataset &ds, std::string &err) {

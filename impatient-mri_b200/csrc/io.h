@@ -28,6 +28,19 @@ struct Dataset {
 int read_data_file(const std::string &fn, bool v02, DataFile &out, std::string &err);
 int load_input_dir(const std::string &dir, Dataset &ds, std::string &err);
 
+// A sparse matrix read from a Matrix Market coordinate file (c.rmtx), 0-based.
+struct SparseCoo {
+    int rows = 0, cols = 0;
+    std::vector<int> row, col;
+    std::vector<float> val;
+};
+
+// readMtxFile() of kernels/mmio.cpp:668-830: banner "%%MatrixMarket matrix
+// coordinate real|integer|pattern general", '%' comment lines, "rows cols nnz",
+// then nnz lines "i j value" (1-based; pattern files have no value: 1.0).
+// Complex matrices are refused, as by the reference.
+int read_mtx(const std::string &fn, SparseCoo &out, std::string &err);
+
 // "%f\n" per element (kernels/structures.cpp:1165-1175).
 int export_text(const std::string &fn, const float *a, size_t n, std::string &err);
 // Raw float32 array (the Toeplitz out.file / FhD.file layout).

@@ -343,17 +343,18 @@ __global__ void k_crop_acc(float2 *acc, const float2 *big, const float2 *sens,
     }
 }
 
-// q += lambda D^H W D p (optional); partial Re<p, q>
+// q += lambda D^H W D p (pen 1) or lambda C^T W C p (pen 2, y = W C p formed
+// beforehand); partial Re<p, q>
 __global__ void __launch_bounds__(kVB) k_t_tvdot(float2 *q, const float2 *p, const float *w,
-                                                 int N, Grid3 gd, int fd, float lambda,
-                                                 double *dots) {
+                                                 int N, Grid3 gd, int pen, float lambda,
+                                                 RegView reg, double *dots) {
     __shared__ double sh[33];
     if (scal(dots)->done) return;
     double loc = 0.0;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
         float2 v = q[r];
-        if (fd) {
-            const float2 t = dhwd_at(p, w, r, gd);
+        if (pen) {
+            const float2 t = pen == 2 ? reg_ct_at(reg, r) : dhwd_at(p, w, r, gd);
             v.x += lambda * t.x;
             v.y += lambda * t.y;
             q[r] = v;
@@ -535,6 +536,7 @@ void ToepSolver::release() {
         grid_fft_destroy(f);
         *f = GridFft();
     }
+    reg_.release();
     void *bufs[] = {sens_, eph_, fm_, qf_, big_, x_, r_, p_, q_, best_, fhd_, w_, dots_,
                     t_, grid_, qf2_, b1_, tw_};
     for (void *b : bufs)
@@ -575,7 +577,8 @@ cudaError_t ToepSolver::setup(const ToepConfig &cfg, const float *t, const float
                                                             (size_t)C * N_);
         k_eph<<<gridn((size_t)L1 * N_), kVB, 0, st>>>(eph_, fm, N_, L1, tau_, t0_);
         launches_ = 2;
-        return cudaGetLastError();
+        T_TRY(cudaGetLastError());
+        return set_reg();
     }
     release();
     cfg_ = cfg;
@@ -639,7 +642,7 @@ cudaError_t ToepSolver::setup(const ToepConfig &cfg, const float *t, const float
     if (!fast_) T_TRY(grid_fft_create(&gf2_, d0, d1, d2, C));
     T_TRY(grid_fft_create(&gf1_, d0, d1, d2, 1));
     launches_ = 2;
-    return cudaSuccess;
+    return set_reg();
 }
 
 cudaError_t ToepSolver::ensure_grid_plan(const GridSpec &g, GridFft *plan) {
@@ -766,11 +769,47 @@ cudaError_t ToepSolver::apply_aha(const float2 *p, float2 *q) {
     return cudaSuccess;
 }
 
+const int *ToepSolver::done_flag() const {
+    return reinterpret_cast<const int *>(
+        reinterpret_cast<const char *>(dots_ + T_SCAL * kTBlocks) + offsetof(TScal, done));
+}
+
+// -reg takes precedence over -fd (toeplitz/recon.cu:1543-1680)
+cudaError_t ToepSolver::penalty_dot(float2 *q, const float2 *p) {
+    const Grid3 gd{nv[0], nv[1], nv[2]};
+    const int pen = reg_.on() ? 2 : cfg_.fd ? 1 : 0;
+    if (pen == 2) {
+        T_TRY(reg_.apply_cw(p, w_, done_flag(), st_));
+        ++launches_;
+    }
+    k_t_tvdot<<<kTBlocks, kVB, 0, st_>>>(q, p, w_, (int)N_, gd, pen, cfg_.lambda, reg_.view(),
+                                        dots_);
+    return cudaGetLastError();
+}
+
+cudaError_t ToepSolver::set_reg() {
+    if (!cfg_.reg) {
+        if (reg_.on()) {
+            reg_.release();
+            if (g_iter_) cudaGraphExecDestroy(g_iter_);
+            g_iter_ = nullptr;
+        }
+        return cudaSuccess;
+    }
+    const bool was_on = reg_.on();
+    bool moved = false;
+    T_TRY(reg_.set(*cfg_.reg, (int)N_, st_, &moved));
+    if ((moved || !was_on) && g_iter_) {
+        cudaGraphExecDestroy(g_iter_);
+        g_iter_ = nullptr;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t ToepSolver::cg_iteration() {
     const Grid3 gd{nv[0], nv[1], nv[2]};
     T_TRY(apply_aha(p_, q_));
-    k_t_tvdot<<<kTBlocks, kVB, 0, st_>>>(q_, p_, w_, (int)N_, gd, cfg_.fd ? 1 : 0, cfg_.lambda,
-                                        dots_);
+    T_TRY(penalty_dot(q_, p_));
     k_t_update<<<kTBlocks, kVB, 0, st_>>>(x_, r_, p_, q_, (int)N_, dots_);
     k_t_dir<<<kTBlocks, kVB, 0, st_>>>(p_, r_, x_, best_, (int)N_, dots_);
     k_t_finish<<<1, 1, 0, st_>>>(dots_);
@@ -820,8 +859,7 @@ cudaError_t ToepSolver::solve(const float *fhd_r, const float *fhd_i, float *x_r
                                   offsetof(TScal, done),
                               0, sizeof(int), st_));
         T_TRY(apply_aha(x_, q_));
-        k_t_tvdot<<<kTBlocks, kVB, 0, st_>>>(q_, x_, w_, N, gd, cfg_.fd ? 1 : 0, cfg_.lambda,
-                                            dots_);
+        T_TRY(penalty_dot(q_, x_));
         k_t_init<<<kTBlocks, kVB, 0, st_>>>(r_, p_, fhd_, q_, N, dots_);
         k_t_init_finish<<<1, kVB, 0, st_>>>(dots_);
         T_TRY(cudaGetLastError());
@@ -862,7 +900,7 @@ cudaError_t ToepSolver::solve_from(const float *fhd_r, const float *fhd_i, float
                           0, sizeof(int), st_));
     // r = F^H d - A x0; p = r
     T_TRY(apply_aha(x_, q_));
-    k_t_tvdot<<<kTBlocks, kVB, 0, st_>>>(q_, x_, w_, N, gd, cfg_.fd ? 1 : 0, cfg_.lambda, dots_);
+    T_TRY(penalty_dot(q_, x_));
     k_t_init<<<kTBlocks, kVB, 0, st_>>>(r_, p_, fhd_, q_, N, dots_);
     k_t_init_finish<<<1, kVB, 0, st_>>>(dots_);
     T_TRY(cudaGetLastError());
@@ -898,10 +936,9 @@ cudaError_t ToepSolver::apply(const float *p_r, const float *p_i, float *q_r, fl
     k_soa2c<<<gridn(N_), kVB, 0, st_>>>(p_, p_r, p_i, N_);
     T_TRY(cudaMemsetAsync(dots_ + T_SCAL * kTBlocks, 0, sizeof(TScal), st_));
     T_TRY(apply_aha(p_, q_));
-    if (cfg_.fd) {
-        const Grid3 gd{nv[0], nv[1], nv[2]};
+    if (cfg_.fd || reg_.on()) {
         k_fillf<<<gridn(N_), kVB, 0, st_>>>(w_, 1.f, N_);
-        k_t_tvdot<<<kTBlocks, kVB, 0, st_>>>(q_, p_, w_, (int)N_, gd, 1, cfg_.lambda, dots_);
+        T_TRY(penalty_dot(q_, p_));
     }
     k_c2soa<<<gridn(N_), kVB, 0, st_>>>(q_r, q_i, q_, N_);
     return cudaGetLastError();
@@ -930,6 +967,10 @@ imp_status toep_args(const imp_toeplitz_options *o, int nx, int ny, int nz, int 
     if (o->gridOS_Q < 1.f || o->gridOS_Q > 2.f || o->gridOS_FH < 1.f || o->gridOS_FH > 2.f)
         return fail(IMP_ERR_INVALID_ARG, "gridding oversampling factor should be in [1.0,2.0]");
     if (o->cg_num <= 0) return fail(IMP_ERR_INVALID_ARG, "cg_num must be > 0");
+    if (o->reg) {
+        const char *why = imp::sparse_reg_check(*o->reg, nx * ny * nz);
+        if (why[0]) return fail(IMP_ERR_INVALID_ARG, std::string("-reg matrix: ") + why);
+    }
     return IMP_OK;
 }
 
@@ -949,6 +990,15 @@ imp::ToepConfig toep_cfg(const imp_toeplitz_options *o, int nx, int ny, int nz, 
     c.tv = o->enable_tv != 0;
     c.tv_num = o->enable_tv ? o->tv_num : 1;
     c.tv_eps = o->tv_eps;
+    c.reg = o->reg;
+    return c;
+}
+
+// The same configuration without the CG's penalty terms (Q and F^H d).
+imp::ToepConfig toep_cfg_nopen(const imp_toeplitz_options *o, int nx, int ny, int nz, int C,
+                               int M) {
+    imp::ToepConfig c = toep_cfg(o, nx, ny, nz, C, M);
+    c.reg = nullptr;
     return c;
 }
 
@@ -1003,7 +1053,7 @@ imp_status imp_toeplitz_q(imp_context *ctx, const imp_toeplitz_options *opt, flo
         (s = imp::to_device_staged(ctx, t, num_k, &dt, nullptr)))
         return s;
     imp::ToepSolver &ts = solver_q_of(ctx);
-    IMP_CUDA(ts.setup(toep_cfg(opt, nx, ny, nz, 1, num_k), dt, nullptr, nullptr, nullptr,
+    IMP_CUDA(ts.setup(toep_cfg_nopen(opt, nx, ny, nz, 1, num_k), dt, nullptr, nullptr, nullptr,
                       ctx->dev_err, ctx->stream),
              "toeplitz setup");
     const size_t nq = (size_t)ts.segments() * ts.q_elems();
@@ -1048,7 +1098,7 @@ imp_status imp_toeplitz_fhd(imp_context *ctx, const imp_toeplitz_options *opt, f
         (s = imp::to_device_staged(ctx, kdata_i, C * M, &dki, nullptr)))
         return s;
     imp::ToepSolver &ts = solver_of(ctx);
-    IMP_CUDA(ts.setup(toep_cfg(opt, nx, ny, nz, num_coil, num_k), dt, dfm, dsr, dsi,
+    IMP_CUDA(ts.setup(toep_cfg_nopen(opt, nx, ny, nz, num_coil, num_k), dt, dfm, dsr, dsi,
                       ctx->dev_err, ctx->stream),
              "toeplitz setup");
     float *dfr, *dfi;

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "grid_fft.cuh"
+#include "sparse_reg.cuh"
 #include "toep_fft.cuh"
 
 namespace imp {
@@ -40,6 +41,7 @@ struct ToepConfig {
     int tv_num = 1;
     float tv_eps = 1e-6f;
     bool use_graphs = true;
+    const imp_sparse *reg = nullptr;  // -reg roughness matrix (host COO), null = off
 };
 
 class ToepSolver {
@@ -80,10 +82,15 @@ public:
 
 private:
     cudaError_t apply_aha(const float2 *p, float2 *q);  // q = A^H A p (no TV term)
+    // q += lambda (D^H W D | C^T W C) p (when a penalty is on); partial Re<p, q>
+    cudaError_t penalty_dot(float2 *q, const float2 *p);
+    const int *done_flag() const;
+    cudaError_t set_reg();
     cudaError_t cg_iteration();
     cudaError_t ensure_grid_plan(const GridSpec &g, GridFft *plan);
 
     ToepConfig cfg_;
+    SparseReg reg_;            // -reg: C and C^T on the device
     cudaStream_t st_ = nullptr;
     unsigned *err_ = nullptr;
     int L_ = 0;

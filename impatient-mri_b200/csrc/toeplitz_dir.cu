@@ -285,10 +285,12 @@ extern "C" imp_status imp_toeplitz_dir_cli(const char *idir, const char *odir, i
                                            int enable_fd, float fdp, int enable_tv, int tv_num,
                                            int direct, float gridOS_Q, float gridOS_FH,
                                            float ntime_segs, int gpu_id, int reuseQ,
-                                           const char *Qpath, int writeQ) {
+                                           const char *Qpath, int writeQ,
+                                           const imp_sparse *reg) {
     (void)odir;  // the reference writes the Toeplitz outputs into the input directory
     imp_toeplitz_options o;
     imp_toeplitz_options_default(&o);
+    o.reg = reg;
     o.cg_num = cg_num;
     o.enable_fd = enable_fd;
     o.fd_penalizer = fdp;

@@ -148,3 +148,37 @@ def read_dataset(d) -> dict:
         out["sensi_r"][:n] = 1.0
         out["sensi_i"][:n] = 0.0
     return out
+
+
+def write_mtx(fn, rows: int, cols: int, I, J, V) -> None:
+    """A sparse real matrix (0-based coordinates) as a Matrix Market coordinate
+    file (c.rmtx), the format readMtxFile reads (kernels/mmio.cpp:668-830) and
+    matlab_utils/create_sparse_matrix/mmwrite.m writes: 1-based "i j value"
+    lines after a "rows cols nnz" line."""
+    I, J, V = np.asarray(I), np.asarray(J), np.asarray(V, np.float64)
+    with open(fn, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{int(rows)} {int(cols)} {I.size}\n")
+        for i, j, v in zip(I.tolist(), J.tolist(), V.tolist()):
+            f.write(f"{i + 1} {j + 1} {v:.17g}\n")
+
+
+def read_mtx(fn):
+    """(rows, cols, I, J, V) of a Matrix Market coordinate file, 0-based
+    (pattern entries read as 1.0; complex matrices refused)."""
+    with open(fn) as f:
+        banner = f.readline().lower()
+        if not banner.startswith("%%matrixmarket") or "coordinate" not in banner:
+            raise ValueError(f"{fn}: not a Matrix Market coordinate file")
+        if "complex" in banner:
+            raise ValueError(f"{fn}: complex matrices are not supported")
+        pattern = "pattern" in banner
+        line = f.readline()
+        while line.startswith("%") or not line.strip():
+            line = f.readline()
+        rows, cols, nnz = (int(x) for x in line.split()[:3])
+        body = np.loadtxt(f, ndmin=2) if nnz else np.zeros((0, 2 if pattern else 3))
+    I = body[:, 0].astype(np.int64) - 1
+    J = body[:, 1].astype(np.int64) - 1
+    V = np.ones(nnz) if pattern else body[:, 2]
+    return rows, cols, I, J, V

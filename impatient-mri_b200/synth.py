@@ -191,3 +191,36 @@ def make_case(name: str, seed: int | None = None, forward=None, small: bool = Fa
         y = forward(case["x_true"], case["sens"], case)
         case["kdata"] = add_noise(np.asarray(y), 40.0, rng).astype(np.complex64)
     return case
+
+
+def fd_matrix(shape):
+    """Roughness matrix C for -reg: periodic first-order differences
+    (C x)_k = x_i - x_{i+1 (mod n)} along each axis of length > 2, one block of
+    N = prod(shape) rows per axis, stacked; coordinate form (rows, cols, I, J,
+    V), 0-based.  Restates matlab_utils/create_sparse_matrix/
+    createDWithPeriodicBoundary.m (2-D) and createDWithPeriodicBoundary3D.m
+    (3-D) for IMPATIENT's row-major voxel order, as that directory's README
+    prescribes: 2-D images [x][y] (y fastest) give the y block then the x
+    block; 3-D images [y][x][z] (z fastest) give the z, x and y blocks.
+    `shape` is the image in voxel order: (nx, ny) or (ny, nx, nz)."""
+    shape = tuple(int(n) for n in shape)
+    N = int(np.prod(shape))
+    idx = np.arange(N).reshape(shape)
+    Is, Js, Vs = [], [], []
+    row0 = 0
+    for ax in reversed(range(len(shape))):  # fastest axis first
+        if shape[ax] <= 2:
+            continue
+        nxt = np.roll(idx, -1, axis=ax)
+        # MATLAB's spdiags order within a block: the column-major (fastest axis
+        # first) ordering of the rows, which is also the voxel index here
+        r = row0 + idx.ravel()
+        Is += [r, r]
+        Js += [idx.ravel(), nxt.ravel()]
+        Vs += [np.ones(N), -np.ones(N)]
+        row0 += N
+    I = np.concatenate(Is)
+    J = np.concatenate(Js)
+    V = np.concatenate(Vs)
+    order = np.lexsort((I, J))  # column-major entry order, as mmwrite writes a sparse matrix
+    return row0, N, I[order], J[order], V[order]

@@ -141,6 +141,18 @@ imp_status imp_parallel_ift_noalloc(float *idata_r, float *idata_i, const float 
 /* ------------------------------------------------------------------------
  * Recon level: brute-force CG (host or device pointers).
  * ---------------------------------------------------------------------- */
+/* Real sparse matrix in coordinate form, 0-based (the reference's CooMatrix,
+ * kernels/structures.h:927-990, read from c.rmtx by readMtxFile,
+ * kernels/mmio.cpp:668-830).  For -reg it is the roughness matrix C:
+ * rows = B * num_i (B blocks of num_i rows, one per difference direction),
+ * cols = num_i. */
+typedef struct imp_sparse {
+    int rows, cols, nnz;
+    const int *row;      /* [nnz] row indices (host memory) */
+    const int *col;      /* [nnz] column indices (host memory) */
+    const float *val;    /* [nnz] values (host memory) */
+} imp_sparse;
+
 typedef struct imp_bf_options {
     int cg_num;          /* CG iteration number; cg_num-1 updates are made  */
     int enable_fd;       /* finite-difference regularizer (-fd / -fdp)      */
@@ -150,6 +162,10 @@ typedef struct imp_bf_options {
     float tv_eps;        /* TV smoothing, reference FP32 value 1e-6         */
     int use_z;           /* 0: reference 2-D semantics, 1: true 3-D         */
     int nx, ny, nz;      /* TV grid.  0,0,0 = reference sqrt(N) x sqrt(N)   */
+    const imp_sparse *reg;  /* -reg: roughness matrix C; NULL = off.  When set,
+                             * lambda C^T W C replaces lambda D^H W D (the
+                             * reference gives -reg precedence over -fd,
+                             * bruteForce/bruteForceCpu.cpp:306-380) */
 } imp_bf_options;
 
 /* Fills `opt` with the reference defaults (main.cpp:96-101). */
@@ -227,7 +243,7 @@ imp_status imp_dataset_info(const char *idir, int *num_k, int *num_i, int *num_c
 
 typedef struct imp_toeplitz_options {
     int cg_num;          /* CG iterations (-cg_num) */
-    int enable_fd;       /* finite-difference regularization (-reg) */
+    int enable_fd;       /* finite-difference regularization (-fd / -fdp) */
     float fd_penalizer;  /* lambda (-fdp) */
     int enable_tv;       /* TV reweighting passes (-tv) */
     int tv_num;          /* TV passes (-tv_num) */
@@ -235,6 +251,9 @@ typedef struct imp_toeplitz_options {
     float ntime_segs;    /* L (-ntime_segs); segments l = 0..(int)L */
     float gridOS_Q;      /* oversampling of the Q gridding (-gridOS_Q) */
     float gridOS_FH;     /* oversampling of the F^H d gridding (-gridOS_FH) */
+    const imp_sparse *reg;  /* -reg: roughness matrix C (NULL = off); lambda
+                             * C^T W C replaces lambda D^H W D in A^H A
+                             * (toeplitz/recon.cu:1543-1673) */
 } imp_toeplitz_options;
 
 /* Defaults of main.cpp:103-444 for the Toeplitz flags. */

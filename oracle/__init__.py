@@ -240,6 +240,34 @@ def ref_bf_cg(case, x0=None, kind="bf64", cg_num=None, lam=None, tv=None, tv_num
     return xr + 1j * xi
 
 
+def ref_bf_cg_reg(case, reg, kind="bf64", cg_num=None, lam=0.0, tv=False, tv_num=1):
+    """The reference's bruteForceCpu with -reg: reg = (rows, cols, I, J, V),
+    0-based coordinates of the roughness matrix C."""
+    L = ref(kind)
+    rows, cols, I, J, V = reg
+    o = case["opts"]
+    cg_num = o["cg_num"] if cg_num is None else cg_num
+    M, N = case["kx"].size, case["ix"].size
+    C = case["sens"].size // N
+    (kx, pkx), (ky, pky), (kz, pkz), (t, pt), (ix, pix), (iy, piy), (iz, piz) = _traj(case)
+    fm, pfm = _d(case["fm"])
+    (sr, psr), (si, psi) = _sens(case["sens"], C, N)
+    y = case["kdata"].reshape(C * M)
+    yr, pyr = _d(y.real)
+    yi, pyi = _d(y.imag)
+    xr = np.zeros(N)
+    xi = np.zeros(N)
+    Ii = np.ascontiguousarray(I, np.int32)
+    Jj = np.ascontiguousarray(J, np.int32)
+    Vv, pv = _d(V)
+    IP = ctypes.POINTER(ctypes.c_int)
+    L.ref_bf_cg_reg(xr.ctypes.data_as(_P), xi.ctypes.data_as(_P), pyr, pyi, pkx, pky, pkz, pix,
+                    piy, piz, pfm, pt, M, N, psr, psi, C, int(cg_num), ctypes.c_double(lam),
+                    1 if tv else 0, int(tv_num if tv else 1), int(rows), int(cols), int(Ii.size),
+                    Ii.ctypes.data_as(IP), Jj.ctypes.data_as(IP), pv)
+    return xr + 1j * xi
+
+
 def ref_recon_dir(idir, cg_num, lam=None, tv=False, tv_num=10, kind="bf64"):
     L = ref(kind)
     nk, ni, nc, ns = (ctypes.c_int() for _ in range(4))

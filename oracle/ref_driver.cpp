@@ -169,4 +169,31 @@ void ref_bf_cg(double *x_r, double *x_i, const double *kd_r, const double *kd_i,
     for (int i = 0; i < num_i; ++i) { x_r[i] = xr[i]; x_i[i] = xi[i]; }
 }
 
+// The same with -reg: the roughness matrix C (COO, 0-based) replaces the
+// finite-difference term (bruteForceCpu.cpp:306-380).
+void ref_bf_cg_reg(double *x_r, double *x_i, const double *kd_r, const double *kd_i,
+                   const double *kx, const double *ky, const double *kz,
+                   const double *ix, const double *iy, const double *iz,
+                   const double *fm, const double *t, int num_k, int num_i,
+                   const double *s_r, const double *s_i, int num_coil,
+                   int cg_num, double fdp, int tv, int tv_num,
+                   int c_rows, int c_cols, int c_nnz, const int *c_i, const int *c_j,
+                   const double *c_v) {
+    ensure_timer();
+    std::vector<DataTraj> kt(num_k), it(num_i);
+    fill_traj(kt.data(), kx, ky, kz, num_k);
+    fill_traj(it.data(), ix, iy, iz, num_i);
+    auto xr = to_ft(x_r, num_i), xi = to_ft(x_i, num_i);
+    auto kr = to_ft(kd_r, num_k * num_coil), ki = to_ft(kd_i, num_k * num_coil);
+    auto f = to_ft(fm, num_i), tt = to_ft(t, num_k);
+    auto sr = to_ft(s_r, num_i * num_coil), si = to_ft(s_i, num_i * num_coil);
+    auto cv = to_ft(c_v, c_nnz);
+    CooMatrix c(c_rows, c_cols, c_nnz, c_i, c_j, cv.data());
+    FLOAT_T *pxr = xr.data(), *pxi = xi.data();
+    bruteForceCpu(&pxr, &pxi, kr.data(), ki.data(), kt.data(), it.data(), f.data(), tt.data(), &c,
+                  cg_num, num_k, num_i, true, false, (FLOAT_T)fdp, tv != 0, tv_num,
+                  sr.data(), si.data(), num_coil);
+    for (int i = 0; i < num_i; ++i) { x_r[i] = xr[i]; x_i[i] = xi[i]; }
+}
+
 }  // extern "C"

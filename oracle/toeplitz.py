@@ -301,6 +301,20 @@ def dhwd(p, w, lam):
     return lam * s
 
 
+def reg_penalty(v, reg, w, lam):
+    """lambda C^T (W (C v)) for -reg (toeplitz/recon.cu:1543-1673): reg =
+    (rows, cols, I, J, V) 0-based coordinates of the real roughness matrix C,
+    W = w applied to every block of N rows."""
+    rows, cols, I, J, V = reg
+    x = np.asarray(v).ravel()
+    y = np.zeros(rows, np.complex128)
+    np.add.at(y, np.asarray(I), np.asarray(V, np.float64) * x[np.asarray(J)])
+    y *= np.tile(np.asarray(w, np.float64).ravel(), rows // x.size)
+    out = np.zeros(x.size, np.complex128)
+    np.add.at(out, np.asarray(J), np.asarray(V, np.float64) * y[np.asarray(I)])
+    return lam * out.reshape(np.shape(v))
+
+
 def tv_weight(x, eps):
     s = np.zeros(x.shape)
     for ax in range(x.ndim):
@@ -311,10 +325,11 @@ def tv_weight(x, eps):
 
 
 def toeplitz_cg(fhd, Q, sens, fm, t, L, cg_num, lam=None, tv=False, tv_num=1, eps=1e-6,
-                tol=1e-16):
+                tol=1e-16, reg=None):
     """toeplitz_recon (recon.cu:1724-2191): CG on (A^H A + lambda D^H W D) x =
     F^H d from x = 0, x carried over TV passes, best-residual iterate
-    returned.  Images in voxel order."""
+    returned; with reg (the -reg roughness matrix) lambda C^T W C replaces the
+    finite-difference term.  Images in voxel order."""
     tau, t0 = time_segments(t, L)
     shape = fhd.shape
     fm = np.asarray(fm, np.float64).reshape(shape)
@@ -327,7 +342,9 @@ def toeplitz_cg(fhd, Q, sens, fm, t, L, cg_num, lam=None, tv=False, tv_num=1, ep
 
     def A(v):
         out = aha(v, Qf, sens, fm, tau, t0)
-        if lam is not None:
+        if reg is not None:  # -reg takes precedence over -fd
+            out = out + reg_penalty(v, reg, w, lam or 0.0)
+        elif lam is not None:
             out = out + dhwd(v, w, lam)
         return out
 

@@ -3,10 +3,13 @@ with torch on the CPU in float64 (no counterpart in the reference, which has
 no learned component).
 
 Used only by tests/ to check the CUDA network's forward pass and gradients.
-With ``emulate_bf16`` the oracle rounds the weights, the packed input and every
-stored activation to bfloat16 exactly where the CUDA network stores BF16, so
-that the comparison isolates the FP32-versus-FP64 accumulation; without it the
-oracle is the exact float64 network.
+With ``emulate_bf16`` the oracle rounds to bfloat16 exactly where the CUDA
+network stores BF16: the weights, the packed input and every stored activation
+on the forward pass, and on the backward pass every layer's output gradient
+after the ReLU mask (the operand the weight, bias and input gradients are
+computed from, k_dz in the CUDA network), so that the comparison isolates the
+FP32-versus-FP64 accumulation; without it the oracle is the exact float64
+network.
 
 Parameter layout (flat float32, as imp_unet_get_params): for every layer the
 weights [cout][ky][kx][cin] then the bias [cout].
@@ -56,14 +59,33 @@ def forward(params, x, H: int, W: int, emulate_bf16: bool = True, torch=None,
         import torch  # noqa: F811
     import torch.nn.functional as F
     layers = unpack(params, torch)
+
+    def bf(t):
+        return t.to(torch.bfloat16).to(torch.float64) if emulate_bf16 else t
+
+    # The network computes with BF16 copies of its FP32 weights and returns the
+    # gradient with respect to those copies in FP32: the rounded weights are
+    # the leaves, so that autograd does not round their gradients back through
+    # the dtype cast.
     leaves = []
     for w, b in layers:
+        w = bf(w).detach()
         w.requires_grad_(requires_grad)
         b.requires_grad_(requires_grad)
         leaves.append((w, b))
 
-    def bf(t):
-        return t.to(torch.bfloat16).to(torch.float64) if emulate_bf16 else t
+    class GradBF16(torch.autograd.Function):
+        """Identity whose backward rounds the incoming gradient to BF16."""
+
+        @staticmethod
+        def forward(ctx, t):
+            return t.view_as(t)
+
+        @staticmethod
+        def backward(ctx, g):
+            return g.to(torch.bfloat16).to(torch.float64)
+
+    gbf = GradBF16.apply if emulate_bf16 else (lambda t: t)
 
     B = x.shape[0]
     x = torch.as_tensor(np.asarray(x, np.float64)).reshape(B, 2, H, W)
@@ -74,7 +96,7 @@ def forward(params, x, H: int, W: int, emulate_bf16: bool = True, torch=None,
     def conv(i, h, last=False):
         w, b = leaves[i]
         ci, co, k, relu = CFG[i]
-        y = F.conv2d(h, bf(w), b, padding=k // 2)
+        y = gbf(F.conv2d(h, w, b, padding=k // 2))
         if relu:
             y = F.relu(y)
         return y if last else bf(y)

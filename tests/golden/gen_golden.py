@@ -17,6 +17,11 @@ Fixtures:
   bf_2d_tv_long.npz  bruteForceCpu, 64x64, 1 coil, 4 x 1024 spiral, cg_num 6,
                   -fdp 1e-3, -tv_num 3: a configuration whose CG iterates amplify
                   rounding-level perturbations (used for reported comparisons)
+  bf_2d_reg.npz   bruteForceCpu with -reg, 32x32, 2 coils, cg_num 4, -fdp 1e-2,
+                  -tv_num 2: the roughness matrix is the periodic difference
+                  matrix of synth.fd_matrix with every entry scaled by a seeded
+                  factor in [0.5, 1.5] (a generic C, not the FD stencil),
+                  stored with the fixture (C_rows, C_cols, C_I, C_J, C_V)
 
 The short runs are chosen so that a 1e-9 relative perturbation of the CG step
 moves the FP64 result by less than 1e-6; longer TV runs amplify such
@@ -90,6 +95,17 @@ def main() -> int:
                             x64=oracle.ref_bf_cg(case, kind="bf64", **kw),
                             x32=oracle.ref_bf_cg(case, kind="bf32", **kw))
         print("wrote", name)
+    case, rng = small_case(32, 2, 4, 256, 24)
+    from impatient_mri_b200 import synth
+    rows, cols, I, J, V = synth.fd_matrix((32, 32))
+    V = V * rng.uniform(0.5, 1.5, V.size)
+    reg = (rows, cols, I, J, V)
+    kw = dict(cg_num=4, lam=1e-2, tv=True, tv_num=2)
+    np.savez_compressed(OUT / "bf_2d_reg.npz", **arrays(case), C_rows=rows, C_cols=cols, C_I=I,
+                        C_J=J, C_V=V, cg_num=kw["cg_num"], lam=kw["lam"], tv_num=kw["tv_num"],
+                        x64=oracle.ref_bf_cg_reg(case, reg, kind="bf64", **kw),
+                        x32=oracle.ref_bf_cg_reg(case, reg, kind="bf32", **kw))
+    print("wrote bf_2d_reg")
     return 0
 
 

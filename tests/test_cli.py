@@ -19,7 +19,7 @@ def run(pkg, *args):
     (("-idir", "x", "-ntime_segs", "4"), "toeplitz flag is not found"),
     (("-idir", "x", "-reuseQ", "q"), "-reuseQ flag requires"),
     (("-idir", "x", "-bogus"), "Unknown option"),
-    (("-idir", "x", "-reg"), "not provided"),
+    (("-idir", "x", "-reg"), "c.rmtx not found"),
     (("-idir", "x", "-cpu"), "no CPU reconstruction path"),
 ])
 def test_flag_errors(pkg, args, msg):

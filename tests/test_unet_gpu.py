@@ -1,10 +1,13 @@
 """The learned warm start's BF16 U-Net on the GPU against its float64 torch-CPU
 oracle (oracle/unet.py), through the C-ABI.
 
-Tolerances (relative L2): the forward pass within 1e-2 of the oracle that
-rounds to BF16 where the network stores BF16 (the rest is FP32 versus FP64
-accumulation); the loss within 1e-2 and every layer's weight gradient within
-1e-1 (the backward pass also carries BF16 output gradients into the GEMMs)."""
+Tolerances (relative L2): with random weights, the forward pass within 1e-2 of
+the oracle that rounds to BF16 where the network stores BF16, the loss within
+1e-2 and every layer's weight gradient within 1e-1 (FP32-versus-FP64
+accumulation moves values across BF16 rounding boundaries, and 18 layers
+amplify those flips); with integer weights and data, where every sum is exact
+(test_gradients_exact_arithmetic), the forward within 1e-6 and every layer's
+weight and bias gradient within 1e-5."""
 import numpy as np
 import pytest
 
@@ -84,6 +87,66 @@ def test_gradients_match_oracle(pkg, ctx):
     print(f"loss {loss:.6f} vs {loss_o:.6f}; layer weight-gradient errors "
           + " ".join(f"{e:.1e}" for e in errs))
     assert worst < 1e-1
+
+
+def exact_params(seed):
+    """Weights in {-1, 0, +1} (each tap non-zero with probability ~2 / fan-in,
+    so activations neither die out nor grow past 2^24), biases in {-1, 0, 1}."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for i, (ci, co, k, _) in enumerate(U.CFG):
+        fan = k * k * (2 if i == 0 else ci)
+        q = min(1.0, 2.5 / fan)
+        w = rng.choice([-1.0, 0.0, 1.0], size=co * k * k * ci, p=[q / 2, 1 - q, q / 2])
+        parts += [w, rng.integers(-1, 2, co).astype(np.float64)]
+    return np.concatenate(parts).astype(np.float32)
+
+
+def test_gradients_exact_arithmetic(pkg, ctx):
+    """A gradient check without rounding noise: integer weights, inputs and
+    targets and a power-of-two pixel count make every FP32 sum of the forward
+    and backward passes exact, so the GPU and the BF16-emulating float64
+    oracle round identical values to BF16 at identical points (activations,
+    output gradients) and break pooling ties alike (first maximum).  Any
+    difference is then an error of the kernels: forward within 1e-6, every
+    layer's weight and bias gradient within 1e-5 (FP32 rounding of the final
+    weight-gradient sums only)."""
+    B, H, W = 2, 32, 32
+    rng = np.random.default_rng(5)
+    x = rng.integers(-4, 5, (B, 2, H * W)).astype(np.float32)
+    t = rng.integers(-4, 5, (B, 2, H * W)).astype(np.float32)
+    p = exact_params(17)
+    net = pkg.UNet(ctx, B, H, W, seed=1)
+    try:
+        net.set_params(p)
+        y = net.forward(x, np.zeros_like(x))
+        loss, g = net.gradients(x, t)
+    finally:
+        net.close()
+    want, _ = U.forward(p, x, H, W, emulate_bf16=True)
+    loss_o, g_o = U.loss_and_grads(p, x, t, H, W, emulate_bf16=True)
+    ef = rel(y, want.detach().numpy())
+    errs = []
+    for i, (a, b) in enumerate(U.layer_slices()):
+        ci, co, k, _ = U.CFG[i]
+        wa, wb, ba, bb = a, b, b, b + co
+        got_w, ref_w = g[wa:wb], g_o[wa:wb]
+        if i == 0:  # the two real input channels
+            got_w = got_w.reshape(co, k * k, ci)[:, :, :2]
+            ref_w = ref_w.reshape(co, k * k, ci)[:, :, :2]
+        got_b, ref_b = g[ba:bb], g_o[ba:bb]
+        if i == len(U.CFG) - 1:  # outputs 0 and 1 of the last layer
+            got_w, ref_w = got_w.reshape(co, ci)[:2], ref_w.reshape(co, ci)[:2]
+            got_b, ref_b = got_b[:2], ref_b[:2]
+        ew = rel(got_w, ref_w) if np.linalg.norm(ref_w) > 0 else float(np.abs(got_w).max())
+        eb = rel(got_b, ref_b) if np.linalg.norm(ref_b) > 0 else float(np.abs(got_b).max())
+        errs.append(max(ew, eb))
+    print(f"exact arithmetic: forward {ef:.1e}, loss {loss:.6f} vs {loss_o:.6f}, layer "
+          f"gradient errors " + " ".join(f"{e:.1e}" for e in errs))
+    assert np.abs(y).max() < 2 ** 20  # the exactness premise
+    assert ef < 1e-6
+    assert abs(loss - loss_o) <= 1e-6 * loss_o
+    assert max(errs) < 1e-5
 
 
 def test_training_reduces_loss(pkg, ctx):
