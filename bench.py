@@ -164,23 +164,35 @@ def rel_l2(a, b):
 
 # ------------------------------------------------------------ reference --
 
-def cpu_reference_sample(case, sample_k: int):
-    """Times the reference's own CPU NUDFT (FP32 + OpenMP build of
-    kernels/ftCpu.cpp via parallelFtCpu) on `sample_k` samples x all voxels x
-    all coils and extrapolates to one reconstruction.  The reference brute
-    force has only the 2-D phase (z constant), so the per-pair work is the
-    same as the 3-D formula's but the values are not the 3-D ones."""
+def cpu_reference_sample(case, sample_k: int, sample_v: int = 512):
+    """Times the reference's own CPU NUDFT pair (FP32 + OpenMP build of
+    kernels/ftCpu.cpp through parallelFtCpu / parallelIftCpu) on bounded
+    samples and extrapolates to one reconstruction: the forward over
+    `sample_k` samples against all voxels, the adjoint over all samples for
+    `sample_v` voxels (each keeps the loop the reference parallelises whole),
+    each scaled to a full apply; a reconstruction is, per TV pass, 1 + (cg_num
+    - 1) forward and cg_num - 1 adjoint applies.  The reference brute force has
+    only the 2-D phase (z constant), so the per-pair work is the same as the
+    3-D formula's but the values are not the 3-D ones."""
     import oracle
-    L = oracle.ref("bf32_omp")
+    M, N = case["M"], case["N"]
+    C = np.asarray(case["sens"]).size // N
     sub = dict(case, kx=case["kx"][:sample_k], ky=case["ky"][:sample_k],
                kz=case["kz"][:sample_k], t=case["t"][:sample_k])
-    x = case["x_true"]
+    vsel = np.linspace(0, N - 1, sample_v).astype(np.int64)
+    sens = np.asarray(case["sens"]).reshape(C, N)
+    adj = dict(case, ix=case["ix"][vsel], iy=case["iy"][vsel], iz=case["iz"][vsel],
+               fm=case["fm"][vsel], sens=sens[:, vsel])
+    d = np.ones((C, M), np.complex64)
     t0 = time.perf_counter()
-    oracle.ref_parallel_ft(x, sub, kind="bf32_omp")
-    dt = time.perf_counter() - t0
-    del L
-    per_apply = dt * case["M"] / sample_k
-    return per_apply * applies_per_recon(), dt
+    oracle.ref_parallel_ft(case["x_true"], sub, kind="bf32_omp")
+    t1 = time.perf_counter()
+    oracle.ref_parallel_ift(d, adj, kind="bf32_omp")
+    t2 = time.perf_counter()
+    f_full, a_full = (t1 - t0) * M / sample_k, (t2 - t1) * N / sample_v
+    n_f = TV_NUM * (1 + (CG_NUM - 1))
+    n_a = TV_NUM * (CG_NUM - 1)
+    return f_full * n_f + a_full * n_a, (f_full, a_full)
 
 
 # zero-start CG updates to NRMSE <= 1e-3 at the warm-start configuration, measured
@@ -211,36 +223,46 @@ def run_reference_warm(args):
     CPU reconstruction is bruteForceCpu, whose CG makes one F and one F^H
     (parallelFtCpu / parallelIftCpu, kernels/parImagingCpu.cpp:84-147) per
     update plus the initial F^H d.  Each step times the reference's FP32
-    OpenMP build of both on a bounded sample of the samples (all voxels and
-    coils) and extrapolates to the full M and to 1 + 2 x 45 applies (45 =
-    zero-start updates to NRMSE <= 1e-3 on this configuration); the CG vector
-    work (length-N) is below 1e-6 of the NUDFT work and not timed."""
+    OpenMP build of both on bounded samples that keep each loop's inner
+    dimension whole (the forward over a subset of the samples against all
+    voxels, the adjoint over all samples for a subset of the voxels: the
+    reference parallelises the inner loop, so shortening it would time
+    thread start-up instead of arithmetic), extrapolates each to the full
+    problem and to 1 + 2 x 45 applies (45 = zero-start updates to NRMSE <= 1e-3
+    on this configuration); the CG vector work (length-N) is below 1e-6 of
+    the NUDFT work and not timed."""
     import oracle
     if not oracle.ref_available("bf32_omp"):
         print(json.dumps({"impl": "reference",
                           "unavailable": "reference CPU build oracle/_ref missing"}))
         return 0
     c = warm_case()
-    k = 256
-    sub = dict(c, kx=c["kx"][:k], ky=c["ky"][:k], kz=c["kz"][:k], t=c["t"][:k])
+    ks, kv = 64, 256  # forward: samples; adjoint: voxels
+    M, N, C = c["M"], c["N"], c["C"]
+    fwd = dict(c, kx=c["kx"][:ks], ky=c["ky"][:ks], kz=c["kz"][:ks], t=c["t"][:ks])
+    vsel = np.linspace(0, N - 1, kv).astype(np.int64)
+    adj = dict(c, ix=c["ix"][vsel], iy=c["iy"][vsel], iz=c["iz"][vsel], fm=c["fm"][vsel],
+               sens=c["sens"][:, vsel])
     rng = np.random.default_rng(0)
-    d = (rng.standard_normal((c["C"], k)) + 1j * rng.standard_normal((c["C"], k)))
-    vals = []
+    d = (rng.standard_normal((C, M)) + 1j * rng.standard_normal((C, M)))
+    vals, tf, ta = [], [], []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        oracle.ref_parallel_ft(c["x"], sub, kind="bf32_omp")
+        oracle.ref_parallel_ft(c["x"], fwd, kind="bf32_omp")
         t1 = time.perf_counter()
-        oracle.ref_parallel_ift(d, sub, kind="bf32_omp")
+        oracle.ref_parallel_ift(d, adj, kind="bf32_omp")
         t2 = time.perf_counter()
-        scale = c["M"] / k
-        v = (t2 - t1) * scale * (1 + WARM_ZERO_UPDATES) + (t1 - t0) * scale * WARM_ZERO_UPDATES
+        f_full, a_full = (t1 - t0) * M / ks, (t2 - t1) * N / kv
         if i >= args.warmup:
-            vals.append(v)
+            vals.append(a_full * (1 + WARM_ZERO_UPDATES) + f_full * WARM_ZERO_UPDATES)
+            tf.append(f_full)
+            ta.append(a_full)
     value = float(np.mean(vals))
     cores = os.cpu_count()
-    sample = (f"reference parallelFtCpu + parallelIftCpu (FP32, OpenMP {cores} threads) on {k} "
-              f"of {c['M']} samples x {c['N']} voxels x {c['C']} coils per step, extrapolated "
-              f"x{c['M'] // k} per apply and to 1 + 2 x {WARM_ZERO_UPDATES} applies per recon "
+    sample = (f"reference parallelFtCpu (FP32, OpenMP {cores} threads) on {ks} of {M} samples x "
+              f"{N} voxels x {C} coils and parallelIftCpu on {M} samples x {kv} of {N} voxels x "
+              f"{C} coils per step, extrapolated to one full apply each (F {np.mean(tf):.0f} s, "
+              f"F^H {np.mean(ta):.0f} s) and to 1 + 2 x {WARM_ZERO_UPDATES} applies per recon "
               f"(zero-start CG to NRMSE <= 1e-3); spread over {len(vals)} steps: "
               f"{min(vals):.0f} .. {max(vals):.0f} s (std {np.std(vals) / value:.1%})")
     line = {"impl": "reference", "metric": WARM_METRIC, "value": value, "unit": UNIT,
@@ -315,20 +337,22 @@ def run_reference(args, ws, rank):
         print(json.dumps({"impl": "reference",
                           "unavailable": "reference CPU build oracle/_ref missing"}))
         return 0
-    sample_k = 8192
+    sample_k, sample_v = 8192, 8192
     cores = os.cpu_count()
-    vals = []
+    vals, fa = [], []
     for i in range(args.warmup + args.steps):
-        v, _ = cpu_reference_sample(case, sample_k)
+        v, per = cpu_reference_sample(case, sample_k, sample_v)
         if i >= args.warmup:
             vals.append(v)
+            fa.append(per)
     value = float(np.mean(vals))
-    sample = (f"reference bruteForce NUDFT (parallelFtCpu, FP32, OpenMP {cores} threads) on "
-              f"{sample_k} of {case['M']} samples x {case['N']} voxels x 4 coils per step, "
-              f"extrapolated x{case['M'] // sample_k} per apply and x{applies_per_recon()} "
-              f"applies per recon; spread over {len(vals)} steps {min(vals):.0f} .. "
-              f"{max(vals):.0f} s; CG vector work (length N, < 1e-5 of the NUDFT work) not "
-              f"counted")
+    f_full, a_full = np.mean(fa, axis=0)
+    sample = (f"reference parallelFtCpu (FP32, OpenMP {cores} threads) on {sample_k} of "
+              f"{case['M']} samples x {case['N']} voxels x 4 coils and parallelIftCpu on all "
+              f"samples x {sample_v} voxels per step, each extrapolated to a full apply "
+              f"(F {f_full:.1f} s, F^H {a_full:.1f} s), x 160 F + 150 F^H per recon; spread "
+              f"over {len(vals)} steps {min(vals):.0f} .. {max(vals):.0f} s; CG vector work "
+              f"(length N, < 1e-5 of the NUDFT work) not counted")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
@@ -495,12 +519,13 @@ def run_ours(args, ws, rank, local, emit=True):
         try:
             import oracle
             if oracle.ref_available("bf32_omp"):
-                v, dt = cpu_reference_sample(case, 8192)
+                v, (f_full, a_full) = cpu_reference_sample(case, 8192, 8192)
                 out["cpu_baseline"] = {
                     "value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                    "sample": (f"reference parallelFtCpu (FP32, OpenMP) on 8192 of {M} samples x "
-                               f"{N} voxels x {C} coils ({dt:.1f} s), extrapolated to "
-                               f"{applies_per_recon()} applies per recon")}
+                    "sample": (f"reference parallelFtCpu on 8192 of {M} samples x {N} voxels and "
+                               f"parallelIftCpu on {M} samples x 8192 voxels, {C} coils (FP32, "
+                               f"OpenMP), each extrapolated to a full apply (F {f_full:.1f} s, "
+                               f"F^H {a_full:.1f} s), x 160 F + 150 F^H per recon")}
         except Exception as e:  # the baseline is reported, never required
             out["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(),
                                    "kind": "reference", "sample": f"failed: {e}"}
