@@ -120,13 +120,14 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def ncu_traffic():
-    """DRAM bytes per NUDFT launch from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "nudft_bf3d_64x64x16.md"
+def ncu_traffic(name="nudft_bf3d_64x64x16.md", key="traffic_bytes_per_launch:"):
+    """DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum of one ncu
+    capture) per launch / application from a committed ncu summary, if any."""
+    p = ROOT / "profiles" / name
     if not p.exists():
         return None
     for ln in p.read_text().splitlines():
-        if ln.strip().startswith("traffic_bytes_per_launch:"):
+        if ln.strip().startswith(key):
             try:
                 return float(ln.split(":", 1)[1].strip().split()[0])
             except ValueError:
@@ -1225,7 +1226,11 @@ def run_headline(args, ws, rank, local):
                 "d2h_bytes_per_step": int(hx.numel() * 4)},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
+                     "frac": achieved / hbm,
+                     "traffic": ncu_traffic("toeplitz_apply_warm512.md",
+                                            "traffic_bytes_per_apply:"),
+                     "traffic_source": "profiles/toeplitz_apply_warm512.md: DRAM bytes of the "
+                                       "three engine kernels of one application (ncu)",
                      "kernel": "one CG update (A^H A application: k_fwd_plane, k_slow with x Qf, "
                                "k_inv_plane with the coil sum; FD term; vector updates); bytes "
                                "= the zero-padded FFT model of one A^H A application",
