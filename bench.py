@@ -1614,7 +1614,8 @@ def main() -> int:
     ap.add_argument("--ref-tv", action="store_true", help="reference-gpu: add -tv -tv_num 10")
     ap.add_argument("--ref-timeout", type=int, default=1200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--slices", type=int, default=4, help="batch384: slices timed")
+    ap.add_argument("--slices", type=int, default=64,
+                    help="batch384: slices timed (all 64 by default: the configuration)")
     ap.add_argument("--workload", default=WARM, choices=[WARM, BF3D, C1, TOEP, BATCH],
                     help="warm512 (default, the metric: learned warm start vs plain CG at "
                          "512x512 with 32 coils, with the brute-force 3-D NUDFT block), "

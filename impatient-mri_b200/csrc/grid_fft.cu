@@ -138,13 +138,19 @@ __device__ __forceinline__ float2 twid(const float2 *__restrict__ tw, int e, boo
     return w;
 }
 
-// Tile geometry of one axis pass: element (c, j) of line c of the tile sits at
-// c * cs + j * js in each shared buffer.
+// Tile geometry of one axis pass: element j of line c of the tile sits at
+// c * rs + j + j / 16 of each shared buffer.  The skew (one pad element per 16)
+// spreads a stage's stride-R writes over the banks; the row stride rs is
+// chosen on the host so that the lines a half-warp touches at once fall on
+// different banks too.
 struct Tile {
-    int n, cw, lcw, cs, js;
+    int n, ln, cw, lcw, rs;
 };
 
-template <int R, bool INV>
+__device__ __forceinline__ int sx(const Tile &g, int c, int j) { return c * g.rs + j + (j >> 4); }
+
+// P2: n is a power of two (so is every Ns), index arithmetic by shifts and masks.
+template <int R, bool INV, bool P2>
 __device__ __forceinline__ void stage(const float2 *__restrict__ A, float2 *__restrict__ B,
                                       const Tile &g, int Ns, const float2 *__restrict__ tw) {
     const int T = g.n / R;
@@ -152,20 +158,18 @@ __device__ __forceinline__ void stage(const float2 *__restrict__ A, float2 *__re
     const int items = T << g.lcw;
     for (int it = threadIdx.x; it < items; it += blockDim.x) {
         const int c = it & (g.cw - 1), i = it >> g.lcw;
-        const int k = i % Ns;
-        const float2 *a = A + c * g.cs;
+        const int k = P2 ? (i & (Ns - 1)) : i % Ns;
         float2 v[R];
 #pragma unroll
-        for (int r = 0; r < R; ++r) v[r] = a[(i + r * T) * g.js];
+        for (int r = 0; r < R; ++r) v[r] = A[sx(g, c, i + r * T)];
         if (k) {
 #pragma unroll
             for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twid(tw, r * k * tstep, INV));
         }
         dft<R, INV>(v);
-        float2 *b = B + c * g.cs;
         const int j0 = (i - k) * R + k;
 #pragma unroll
-        for (int q = 0; q < R; ++q) b[(j0 + q * Ns) * g.js] = v[q];
+        for (int q = 0; q < R; ++q) B[sx(g, c, j0 + q * Ns)] = v[q];
     }
 }
 
@@ -182,31 +186,33 @@ __device__ __forceinline__ void stage_generic(const float2 *__restrict__ A, floa
         const int q = rem / Ns, k = rem % Ns;
         const int i = blk * Ns + k;
         const int step = k * tstep + q * rstep;
-        const float2 *a = A + c * g.cs;
         float2 acc = make_float2(0.f, 0.f);
         int e = 0;
         for (int r = 0; r < R; ++r) {
-            const float2 u = cmul(a[(i + r * T) * g.js], twid(tw, e, INV));
+            const float2 u = cmul(A[sx(g, c, i + r * T)], twid(tw, e, INV));
             acc.x += u.x;
             acc.y += u.y;
             e += step;
             if (e >= n) e -= n * (e / n);
         }
-        B[c * g.cs + o * g.js] = acc;
+        B[sx(g, c, o)] = acc;
     }
 }
 
 struct AxisArgs {
     long long S;       // element stride of the axis (product of the faster lengths)
-    int n, cw, lcw;    // axis length, lines per block (power of two), log2(cw)
+    int n, ln;         // axis length and its log2 (when a power of two)
+    int cw, lcw, rs;   // lines per block (power of two), log2(cw), tile row stride
     int nst;           // stages
     unsigned char rad[24];
 };
 
+constexpr int kLoadUnroll = 4;  // global loads a thread issues before its shared stores
+
 // One axis pass.  Block b takes lines l0 = b cw .. l0 + cw - 1 (line l = o S + i
 // starts at o n S + i): consecutive columns of a strided axis (cw divides S),
 // consecutive whole lines of the contiguous one (S = 1).
-template <bool INV>
+template <bool INV, bool P2>
 __global__ void __launch_bounds__(kThreads) k_fft_axis(float2 *__restrict__ data, AxisArgs p,
                                                        const float2 *__restrict__ tw) {
     extern __shared__ float2 sm[];
@@ -214,26 +220,48 @@ __global__ void __launch_bounds__(kThreads) k_fft_axis(float2 *__restrict__ data
     const bool contig = p.S == 1;
     Tile g;
     g.n = n;
+    g.ln = p.ln;
     g.cw = p.cw;
     g.lcw = p.lcw;
-    g.cs = contig ? n + 1 : 1;
-    g.js = contig ? 1 : p.cw;
-    const int buf = contig ? p.cw * (n + 1) : p.cw * n;
-    float2 *A = sm, *B = sm + buf;
+    g.rs = p.rs;
+    float2 *A = sm, *B = sm + p.cw * p.rs;
     const long long l0 = (long long)blockIdx.x * p.cw;
     const int E = n << p.lcw;
-    if (contig) {
-        const float2 *src = data + l0 * n;
-        for (int e = threadIdx.x; e < E; e += blockDim.x) {
-            const int c = e / n, j = e - c * n;
-            A[c * g.cs + j] = src[e];
+    const int step = blockDim.x * kLoadUnroll;
+    // line and element of flat tile index e (contiguous: line-major; strided: column-major)
+    auto split = [&](int e, int &c, int &j) {
+        if (contig) {
+            c = P2 ? e >> p.ln : e / n;
+            j = e - c * n;
+        } else {
+            c = e & (p.cw - 1);
+            j = e >> p.lcw;
         }
-    } else {
-        const long long o = l0 / p.S, i0 = l0 - o * p.S;
-        const float2 *src = data + o * n * p.S + i0;
-        for (int e = threadIdx.x; e < E; e += blockDim.x) {
-            const int c = e & (p.cw - 1), j = e >> p.lcw;
-            A[j * g.js + c] = src[(long long)j * p.S + c];
+    };
+    const long long o = contig ? 0 : l0 / p.S, i0 = contig ? 0 : l0 - o * p.S;
+    float2 *base = contig ? data + l0 * n : data + o * n * p.S + i0;
+    auto gaddr = [&](int e, int c, int j) -> long long {
+        return contig ? (long long)e : (long long)j * p.S + c;
+    };
+    for (int e0 = threadIdx.x; e0 < E; e0 += step) {
+        float2 v[kLoadUnroll];
+#pragma unroll
+        for (int u = 0; u < kLoadUnroll; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e < E) {
+                int c, j;
+                split(e, c, j);
+                v[u] = base[gaddr(e, c, j)];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kLoadUnroll; ++u) {
+            const int e = e0 + u * blockDim.x;
+            if (e < E) {
+                int c, j;
+                split(e, c, j);
+                A[sx(g, c, j)] = v[u];
+            }
         }
     }
     __syncthreads();
@@ -241,13 +269,13 @@ __global__ void __launch_bounds__(kThreads) k_fft_axis(float2 *__restrict__ data
     for (int s = 0; s < p.nst; ++s) {
         const int R = p.rad[s];
         switch (R) {
-            case 2: stage<2, INV>(A, B, g, Ns, tw); break;
-            case 3: stage<3, INV>(A, B, g, Ns, tw); break;
-            case 4: stage<4, INV>(A, B, g, Ns, tw); break;
-            case 5: stage<5, INV>(A, B, g, Ns, tw); break;
-            case 7: stage<7, INV>(A, B, g, Ns, tw); break;
-            case 8: stage<8, INV>(A, B, g, Ns, tw); break;
-            case 16: stage<16, INV>(A, B, g, Ns, tw); break;
+            case 2: stage<2, INV, P2>(A, B, g, Ns, tw); break;
+            case 3: stage<3, INV, P2>(A, B, g, Ns, tw); break;
+            case 4: stage<4, INV, P2>(A, B, g, Ns, tw); break;
+            case 5: stage<5, INV, P2>(A, B, g, Ns, tw); break;
+            case 7: stage<7, INV, P2>(A, B, g, Ns, tw); break;
+            case 8: stage<8, INV, P2>(A, B, g, Ns, tw); break;
+            case 16: stage<16, INV, P2>(A, B, g, Ns, tw); break;
             default: stage_generic<INV>(A, B, g, R, Ns, tw); break;
         }
         __syncthreads();
@@ -256,20 +284,22 @@ __global__ void __launch_bounds__(kThreads) k_fft_axis(float2 *__restrict__ data
         B = t;
         Ns *= R;
     }
-    if (contig) {
-        float2 *dst = data + l0 * n;
-        for (int e = threadIdx.x; e < E; e += blockDim.x) {
-            const int c = e / n, j = e - c * n;
-            dst[e] = A[c * g.cs + j];
-        }
-    } else {
-        const long long o = l0 / p.S, i0 = l0 - o * p.S;
-        float2 *dst = data + o * n * p.S + i0;
-        for (int e = threadIdx.x; e < E; e += blockDim.x) {
-            const int c = e & (p.cw - 1), j = e >> p.lcw;
-            dst[(long long)j * p.S + c] = A[j * g.js + c];
-        }
+    for (int e = threadIdx.x; e < E; e += blockDim.x) {
+        int c, j;
+        split(e, c, j);
+        base[gaddr(e, c, j)] = A[sx(g, c, j)];
     }
+}
+
+// Tile row stride for lines of n points, cw lines per block: long enough for
+// the skewed line, and such that the rows a half-warp touches at once (16 / cw
+// elements of each of cw lines, or 16 lines) start on distinct bank pairs.
+int row_stride(int n, int cw) {
+    const int base = n + ((n - 1) >> 4);
+    const int m = cw >= 16 ? 2 : 32 / cw, t = cw >= 16 ? 1 : 16 / cw;
+    int rs = base;
+    while (rs % m != t % m) ++rs;
+    return rs;
 }
 
 // Radices of n: 16s, then 8, 4, 2, then 3, 5, 7, then any other prime.
@@ -322,11 +352,13 @@ cudaError_t grid_fft_create(GridFft *f, int n0, int n1, int n2, int batch) {
     f->batch = batch;
     {  // per device: set on every plan (cheap)
         const int lim = 160 * 1024;
-        cudaError_t e = cudaFuncSetAttribute(k_fft_axis<false>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_fft_axis<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     lim);
+        cudaError_t e = cudaSuccess;
+        for (const void *k : {(const void *)k_fft_axis<false, false>,
+                              (const void *)k_fft_axis<true, false>,
+                              (const void *)k_fft_axis<false, true>,
+                              (const void *)k_fft_axis<true, true>})
+            if (e == cudaSuccess)
+                e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
         if (e != cudaSuccess) return e;
     }
     for (int a = 0; a < 3; ++a) {
@@ -339,14 +371,14 @@ cudaError_t grid_fft_create(GridFft *f, int n0, int n1, int n2, int batch) {
         int cw;
         if (S == 1) {
             cw = pow2_divisor_le(O, std::max(1, std::min(64, 4096 / len)));
-            f->smem[a] = sizeof(float2) * 2 * (size_t)cw * (len + 1);
         } else {
             int cap = std::max(1, std::min(32, 4096 / len));
             if (cap < 4) cap = std::max(1, std::min(4, 8192 / len));
             cw = pow2_divisor_le(S, cap);
-            f->smem[a] = sizeof(float2) * 2 * (size_t)cw * len;
         }
         f->cw[a] = cw;
+        f->rs[a] = row_stride(len, cw);
+        f->smem[a] = sizeof(float2) * 2 * (size_t)cw * f->rs[a];
         std::vector<float2> h(len);
         for (int j = 0; j < len; ++j) {
             const double ang = -2.0 * kPiD * (double)j / (double)len;
@@ -382,16 +414,23 @@ cudaError_t grid_fft_exec(const GridFft &f, float2 *data, bool inverse, cudaStre
         for (int b = a + 1; b < 3; ++b) p.S *= f.n[b];
         for (int b = 0; b < a; ++b) O *= f.n[b];
         p.n = len;
+        p.ln = ilog2i(len);
         p.cw = f.cw[a];
         p.lcw = ilog2i(p.cw);
+        p.rs = f.rs[a];
         p.nst = f.nfac[a];
         for (int s = 0; s < p.nst; ++s) p.rad[s] = f.fac[a][s];
         const long long blocks = O * p.S / p.cw;
         if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
-        if (inverse)
-            k_fft_axis<true><<<(unsigned)blocks, kThreads, f.smem[a], st>>>(data, p, f.tw[a]);
-        else
-            k_fft_axis<false><<<(unsigned)blocks, kThreads, f.smem[a], st>>>(data, p, f.tw[a]);
+        const bool p2 = (len & (len - 1)) == 0;
+        const unsigned nb = (unsigned)blocks;
+        if (inverse) {
+            if (p2) k_fft_axis<true, true><<<nb, kThreads, f.smem[a], st>>>(data, p, f.tw[a]);
+            else k_fft_axis<true, false><<<nb, kThreads, f.smem[a], st>>>(data, p, f.tw[a]);
+        } else {
+            if (p2) k_fft_axis<false, true><<<nb, kThreads, f.smem[a], st>>>(data, p, f.tw[a]);
+            else k_fft_axis<false, false><<<nb, kThreads, f.smem[a], st>>>(data, p, f.tw[a]);
+        }
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

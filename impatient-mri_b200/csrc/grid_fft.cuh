@@ -26,6 +26,7 @@ struct GridFft {
     int nfac[3] = {0, 0, 0};
     unsigned char fac[3][24] = {};                // radix sequence per axis
     int cw[3] = {1, 1, 1};                        // lines per block
+    int rs[3] = {1, 1, 1};                        // shared tile row stride (elements)
     size_t smem[3] = {0, 0, 0};
     size_t elems() const { return (size_t)batch * n[0] * n[1] * n[2]; }
     int passes() const { return (n[0] > 1) + (n[1] > 1) + (n[2] > 1); }  // kernel launches
