@@ -205,7 +205,27 @@ struct AxisArgs {
     int cw, lcw, rs;   // lines per block (power of two), log2(cw), tile row stride
     int nst;           // stages
     unsigned char rad[24];
+    // Pruning.  Outputs kept along this axis: j < klo or j >= n - khi (klo = n:
+    // all).  Lines: only those whose coordinates along the faster axes are kept
+    // there, enumerated compactly: nf faster axes (outer first) with kept
+    // ranges [0, flo) and [fg - fhi, fg); Sc = product of their kept counts.
+    int klo, khi;
+    int nf;
+    int flo[2], fhi[2], fg[2];
+    long long Sc;
 };
+
+// Offset (within S) of compact line index ic over the kept faster coordinates.
+__device__ __forceinline__ long long line_offset(const AxisArgs &p, long long ic) {
+    auto ex = [](long long c, int lo, int hi, int g) -> long long {
+        return c < lo ? c : c + (g - lo - hi);
+    };
+    if (p.nf == 0) return ic;
+    if (p.nf == 1) return ex(ic, p.flo[0], p.fhi[0], p.fg[0]);
+    const long long inner = p.flo[1] + p.fhi[1];
+    const long long y = ic / inner, z = ic - y * inner;
+    return ex(y, p.flo[0], p.fhi[0], p.fg[0]) * p.fg[1] + ex(z, p.flo[1], p.fhi[1], p.fg[1]);
+}
 
 constexpr int kLoadUnroll = 4;  // global loads a thread issues before its shared stores
 
@@ -238,7 +258,10 @@ __global__ void __launch_bounds__(kThreads) k_fft_axis(float2 *__restrict__ data
             j = e >> p.lcw;
         }
     };
-    const long long o = contig ? 0 : l0 / p.S, i0 = contig ? 0 : l0 - o * p.S;
+    // strided: the block's lines are compact indices l0 .. l0 + cw - 1 over (slower
+    // coordinate o, kept faster coordinates); cw divides the innermost kept range
+    const long long o = contig ? 0 : l0 / p.Sc;
+    const long long i0 = contig ? 0 : line_offset(p, l0 - o * p.Sc);
     float2 *base = contig ? data + l0 * n : data + o * n * p.S + i0;
     auto gaddr = [&](int e, int c, int j) -> long long {
         return contig ? (long long)e : (long long)j * p.S + c;
@@ -287,6 +310,7 @@ __global__ void __launch_bounds__(kThreads) k_fft_axis(float2 *__restrict__ data
     for (int e = threadIdx.x; e < E; e += blockDim.x) {
         int c, j;
         split(e, c, j);
+        if (j >= p.klo && j < n - p.khi) continue;  // output cropped away
         base[gaddr(e, c, j)] = A[sx(g, c, j)];
     }
 }
@@ -403,8 +427,25 @@ void grid_fft_destroy(GridFft *f) {
 }
 
 cudaError_t grid_fft_exec(const GridFft &f, float2 *data, bool inverse, cudaStream_t st) {
+    return grid_fft_exec_cropped(f, data, inverse, nullptr, st);
+}
+
+cudaError_t grid_fft_exec_cropped(const GridFft &f, float2 *data, bool inverse,
+                                  const int keep_half[3], cudaStream_t st) {
+    // kept output range per axis: [0, lo) and [n - hi, n)
+    int klo[3], khi[3];
+    for (int a = 0; a < 3; ++a) {
+        const int h = keep_half ? keep_half[a] : 0;
+        if (h > 0 && 2 * h <= f.n[a]) {
+            klo[a] = h;
+            khi[a] = h;
+        } else {
+            klo[a] = f.n[a];
+            khi[a] = 0;
+        }
+    }
     // the fastest axis first: its pass is the one whose reads and writes are
-    // whole contiguous lines
+    // whole contiguous lines; later passes only take lines kept by earlier ones
     for (int a = 2; a >= 0; --a) {
         const int len = f.n[a];
         if (len == 1) continue;
@@ -415,21 +456,42 @@ cudaError_t grid_fft_exec(const GridFft &f, float2 *data, bool inverse, cudaStre
         for (int b = 0; b < a; ++b) O *= f.n[b];
         p.n = len;
         p.ln = ilog2i(len);
-        p.cw = f.cw[a];
-        p.lcw = ilog2i(p.cw);
-        p.rs = f.rs[a];
         p.nst = f.nfac[a];
         for (int s = 0; s < p.nst; ++s) p.rad[s] = f.fac[a][s];
-        const long long blocks = O * p.S / p.cw;
+        p.klo = klo[a];
+        p.khi = khi[a];
+        p.nf = 0;
+        p.Sc = 1;
+        int inner_lo = 0, inner_hi = 0;
+        bool gap = false;
+        for (int b = a + 1; b < 3; ++b) {
+            if (f.n[b] == 1) continue;
+            p.flo[p.nf] = klo[b];
+            p.fhi[p.nf] = khi[b];
+            p.fg[p.nf] = f.n[b];
+            p.Sc *= (long long)(klo[b] + khi[b]);
+            inner_lo = klo[b];
+            inner_hi = khi[b];
+            gap = gap || khi[b] > 0;
+            ++p.nf;
+        }
+        p.cw = f.cw[a];
+        if (p.S > 1 && gap) {  // a block's columns must be consecutive in memory
+            while (p.cw > 1 && (p.Sc % p.cw || inner_lo % p.cw || inner_hi % p.cw)) p.cw >>= 1;
+        }
+        p.lcw = ilog2i(p.cw);
+        p.rs = row_stride(len, p.cw);
+        const size_t smem = sizeof(float2) * 2 * (size_t)p.cw * p.rs;
+        const long long blocks = (p.S > 1 ? O * p.Sc : O) / p.cw;
         if (blocks > 0x7fffffffLL) return cudaErrorInvalidValue;
         const bool p2 = (len & (len - 1)) == 0;
         const unsigned nb = (unsigned)blocks;
         if (inverse) {
-            if (p2) k_fft_axis<true, true><<<nb, kThreads, f.smem[a], st>>>(data, p, f.tw[a]);
-            else k_fft_axis<true, false><<<nb, kThreads, f.smem[a], st>>>(data, p, f.tw[a]);
+            if (p2) k_fft_axis<true, true><<<nb, kThreads, smem, st>>>(data, p, f.tw[a]);
+            else k_fft_axis<true, false><<<nb, kThreads, smem, st>>>(data, p, f.tw[a]);
         } else {
-            if (p2) k_fft_axis<false, true><<<nb, kThreads, f.smem[a], st>>>(data, p, f.tw[a]);
-            else k_fft_axis<false, false><<<nb, kThreads, f.smem[a], st>>>(data, p, f.tw[a]);
+            if (p2) k_fft_axis<false, true><<<nb, kThreads, smem, st>>>(data, p, f.tw[a]);
+            else k_fft_axis<false, false><<<nb, kThreads, smem, st>>>(data, p, f.tw[a]);
         }
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;

@@ -44,4 +44,12 @@ void grid_fft_destroy(GridFft *f);
 // In-place unnormalised transform of `data` (f.elems() complex values).
 cudaError_t grid_fft_exec(const GridFft &f, float2 *data, bool inverse, cudaStream_t st);
 
+// The same transform when only a crop of the output is read afterwards: along
+// axis a, outputs j < keep_half[a] and j >= n[a] - keep_half[a] (0: all).  Each
+// axis pass (fastest first) transforms only the lines whose faster coordinates
+// are kept and stores only its kept outputs; everything else of `data` is left
+// undefined.
+cudaError_t grid_fft_exec_cropped(const GridFft &f, float2 *data, bool inverse,
+                                  const int keep_half[3], cudaStream_t st);
+
 }  // namespace imp

@@ -767,8 +767,15 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
 #undef IMP_PLANE_CASE
     const int r1 = split_r1(p.ns);
     const int cols = p.ncol / p.W;
-    // one block row per coil: enough blocks to fill every SM several times over
-    const dim3 blocks(cols, p.C);
+    // Coils: one block row each when Qf_l of the segment (read by every coil)
+    // stays in L2 anyway (2-D 512x512: 8 MB), which fills the SMs with blocks;
+    // otherwise (3-D 256x256x32: 134 MB) each block loops over its coils so that
+    // Qf_l is read from DRAM once and reused from cache by the later coils.
+    const size_t qf_bytes = (size_t)2 * p.ns * p.ncol * sizeof(float2);
+    const int rows_y = qf_bytes <= (size_t(64) << 20)
+                           ? p.C
+                           : std::max(1, std::min(p.C, (2 * 148 + cols - 1) / cols));
+    const dim3 blocks(cols, rows_y);
     const int threads = p.W * r1;
 #define IMP_SLOW_CASE(NSV)                                                                 \
     case NSV:                                                                              \

@@ -11,8 +11,10 @@
 // B200 design (not a translation of the reference kernels):
 // * gridding is a scatter of each sample's separable KB footprint with vector
 //   float2 atomics straight into the ifftshifted position of the FFT buffer,
-//   for the (at most two) time segments whose Hanning window covers the
-//   sample -- no CPU binning, no overflow path, no host round trips;
+//   one warp per sample (the lanes on contiguous cells), for the (at most two)
+//   time segments whose Hanning window covers the sample -- no CPU binning, no
+//   overflow path, no host round trips; the inverse transform is cropped to the
+//   cells the post kernels read;
 // * every shift / crop / deapodisation / phase / SENSE step is an index map
 //   fused into the kernels around the FFTs; the FFTs are this library's own
 //   (the pruned F^H F engine of toep_fft.cu for power-of-two images, the
@@ -109,56 +111,80 @@ __device__ __forceinline__ float kb_transform(float u, float beta) {
     return 1.f;
 }
 
-// Scatter gridding of one time segment.  Writes cell X to its ifftshifted
-// position (X + gs/2) mod gs, ready for the inverse FFT.
-__global__ void k_grid(float2 *grid, const float *kx, const float *ky, const float *kz,
-                       const float *t, const float *dr, const float *di, int M, GridSpec g,
-                       float tau, float t0, int l) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= M) return;
-    const float h = hanning(t[s], tau, l, t0);
-    if (h == 0.f) return;
-    float vr = h, vi = 0.f;
-    if (dr) {
-        vr = h * dr[s];
-        vi = h * (di ? di[s] : 0.f);
-        if (vr == 0.f && vi == 0.f) return;
-    }
-    const float k3[3] = {kx[s], ky[s], g.is3d ? kz[s] : 0.f};
-    int lo[3], cnt[3];
-    float w[3][kMaxTaps];
+// Scatter gridding of one time segment, one warp per sample: each sample's
+// separable KB footprint is added into the ifftshifted position (X + gs/2) mod
+// gs of every cell X it covers (ready for the inverse FFT).  The lanes take the
+// cells of the footprint's two fastest-varying axes (z and y in 3-D, y and x in 2-D; up to
+// 9 x 9 at OS 2), so one atomic instruction of the warp updates a few
+// contiguous runs of the grid instead of 32 scattered cells, and the outer
+// axis is looped.  The per-axis KB weights are computed once per sample into
+// shared memory.
+constexpr int kGridWarps = 8;
+
+__global__ void __launch_bounds__(kGridWarps * 32)
+    k_grid_w(float2 *grid, const float *kx, const float *ky, const float *kz, const float *t,
+             const float *dr, const float *di, int M, GridSpec g, float tau, float t0, int l) {
+    __shared__ float wsh[kGridWarps][3][kMaxTaps];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    float(&ws)[3][kMaxTaps] = wsh[wid];
     const float inv_os = 1.0f / g.os;
-    for (int a = 0; a < 3; ++a) {
-        if (a == 2 && !g.is3d) {
-            lo[2] = 0;
-            cnt[2] = 1;
-            w[2][0] = 1.f;
-            continue;
+    // loop axis A, lane axes B (slower) and Cc (faster)
+    const int A = g.is3d ? 0 : 2, B = g.is3d ? 1 : 0, Cc = g.is3d ? 2 : 1;
+    for (int s = blockIdx.x * kGridWarps + wid; s < M; s += gridDim.x * kGridWarps) {
+        const float h = hanning(__ldg(&t[s]), tau, l, t0);
+        if (h == 0.f) continue;  // warp-uniform: every lane reads the same sample
+        float vr = h, vi = 0.f;
+        if (dr) {
+            vr = h * __ldg(&dr[s]);
+            vi = h * (di ? __ldg(&di[s]) : 0.f);
+            if (vr == 0.f && vi == 0.f) continue;
         }
-        const float c = g.os * (g.kscale * k3[a] + 0.5f * (float)g.img[a]);
-        const float r = 0.5f * kKW * g.os;
-        int a0 = (int)ceilf(c - r), a1 = (int)floorf(c + r);
-        a0 = max(a0, 0);
-        a1 = min(a1, g.gs[a] - 1);
-        a1 = min(a1, a0 + kMaxTaps - 1);
-        lo[a] = a0;
-        cnt[a] = max(a1 - a0 + 1, 0);
-        for (int j = 0; j < cnt[a]; ++j) w[a][j] = kb_weight(fabsf(c - (float)(a0 + j)) * inv_os, g.beta);
-    }
-    for (int i = 0; i < cnt[0]; ++i) {
-        const int xs = (lo[0] + i + g.gs[0] / 2) % g.gs[0];
-        for (int j = 0; j < cnt[1]; ++j) {
-            const float wxy = w[0][i] * w[1][j];
-            if (wxy == 0.f) continue;
-            const int ys = (lo[1] + j + g.gs[1] / 2) % g.gs[1];
-            const size_t row = ((size_t)xs * g.gs[1] + ys) * g.gs[2];
-            for (int k = 0; k < cnt[2]; ++k) {
-                const float ww = wxy * w[2][k];
+        const float k3[3] = {__ldg(&kx[s]), __ldg(&ky[s]), g.is3d ? __ldg(&kz[s]) : 0.f};
+        int lo[3], cnt[3];
+        float cc[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (a == 2 && !g.is3d) {
+                lo[2] = 0;
+                cnt[2] = 1;
+                cc[2] = 0.f;
+                continue;
+            }
+            const float c = g.os * (g.kscale * k3[a] + 0.5f * (float)g.img[a]);
+            const float r = 0.5f * kKW * g.os;
+            int a0 = (int)ceilf(c - r), a1 = (int)floorf(c + r);
+            a0 = max(a0, 0);
+            a1 = min(a1, g.gs[a] - 1);
+            a1 = min(a1, a0 + kMaxTaps - 1);
+            lo[a] = a0;
+            cnt[a] = max(a1 - a0 + 1, 0);
+            cc[a] = c;
+        }
+        for (int q = lane; q < 3 * kMaxTaps; q += 32) {
+            const int a = q / kMaxTaps, j = q - a * kMaxTaps;
+            if (j < cnt[a])
+                ws[a][j] = (a == 2 && !g.is3d)
+                               ? 1.f
+                               : kb_weight(fabsf(cc[a] - (float)(lo[a] + j)) * inv_os, g.beta);
+        }
+        __syncwarp();
+        const int nbc = cnt[B] * cnt[Cc];
+        for (int p = lane; p < nbc; p += 32) {
+            const int jb = p / cnt[Cc], jc = p - jb * cnt[Cc];
+            const float wbc = ws[B][jb] * ws[Cc][jc];
+            if (wbc == 0.f) continue;
+            int idx[3];
+            idx[B] = (lo[B] + jb + g.gs[B] / 2) % g.gs[B];
+            idx[Cc] = (lo[Cc] + jc + g.gs[Cc] / 2) % g.gs[Cc];
+            for (int ja = 0; ja < cnt[A]; ++ja) {
+                const float ww = wbc * ws[A][ja];
                 if (ww == 0.f) continue;
-                const int zs = g.is3d ? (lo[2] + k + g.gs[2] / 2) % g.gs[2] : 0;
-                atomicAdd(&grid[row + zs], make_float2(ww * vr, ww * vi));
+                idx[A] = g.is3d ? (lo[A] + ja + g.gs[A] / 2) % g.gs[A] : 0;
+                const size_t cell = ((size_t)idx[0] * g.gs[1] + idx[1]) * g.gs[2] + idx[2];
+                atomicAdd(&grid[cell], make_float2(ww * vr, ww * vi));
             }
         }
+        __syncwarp();  // the next sample overwrites ws
     }
 }
 
@@ -500,6 +526,21 @@ float beatty_beta(float os) {
 
 }  // namespace
 
+// The output crop the post kernels read after the inverse transform of a
+// gridding grid, as half-lengths per FFT axis (grid_image_value: along each
+// axis the image's img/2 cells on either side of index 0).
+struct Crop {
+    int v[3];
+};
+static Crop crop_of(const GridSpec &g) {
+    if (g.is3d) return Crop{{g.img[0] / 2, g.img[1] / 2, g.img[2] / 2}};
+    return Crop{{0, g.img[0] / 2, g.img[1] / 2}};
+}
+
+// Blocks of the warp-per-sample gridding: resident blocks of 8 warps on every
+// SM a few times over (grid-stride over the samples).
+static unsigned grid_blocks() { return 148u * 8u; }
+
 GridSpec grid_spec(const int img[3], float os, bool beta_after_rounding, float kscale) {
     GridSpec g;
     for (int a = 0; a < 3; ++a) g.img[a] = img[a];
@@ -670,10 +711,10 @@ cudaError_t ToepSolver::compute_q(const float *kx, const float *ky, const float 
     const NV n2d{{n2[0], n2[1], n2[2]}};
     for (int l = 0; l <= L_; ++l) {
         T_TRY(cudaMemsetAsync(grid_, 0, sizeof(float2) * g.cells(), st_));
-        k_grid<<<(cfg_.M + 127) / 128, 128, 0, st_>>>(grid_, kx, ky, kz, t_, nullptr, nullptr,
-                                                      cfg_.M, g, tau_, t0_, l);
+        k_grid_w<<<grid_blocks(), kGridWarps * 32, 0, st_>>>(grid_, kx, ky, kz, t_, nullptr,
+                                                             nullptr, cfg_.M, g, tau_, t0_, l);
         T_TRY(cudaGetLastError());
-        T_TRY(grid_fft_exec(gfq_, grid_, true, st_));
+        T_TRY(grid_fft_exec_cropped(gfq_, grid_, true, crop_of(g).v, st_));
         float2 *qf_l = fast_ ? qf_ : qf_ + (size_t)l * G2_;
         k_q_post<<<gridn(G2_), kVB, 0, st_>>>(grid_, g, n2d, qf_l,
                                              q_out_r ? q_out_r + (size_t)l * G2_ : nullptr,
@@ -719,11 +760,11 @@ cudaError_t ToepSolver::compute_fhd(const float *kx, const float *ky, const floa
     for (int c = 0; c < cfg_.C; ++c)
         for (int l = 0; l <= L_; ++l) {
             T_TRY(cudaMemsetAsync(grid_, 0, sizeof(float2) * g.cells(), st_));
-            k_grid<<<(cfg_.M + 127) / 128, 128, 0, st_>>>(
+            k_grid_w<<<grid_blocks(), kGridWarps * 32, 0, st_>>>(
                 grid_, kx, ky, kz, t_, kd_r + (size_t)c * cfg_.M, kd_i + (size_t)c * cfg_.M,
                 cfg_.M, g, tau_, t0_, l);
             T_TRY(cudaGetLastError());
-            T_TRY(grid_fft_exec(gff_, grid_, true, st_));
+            T_TRY(grid_fft_exec_cropped(gff_, grid_, true, crop_of(g).v, st_));
             k_fh_post<<<gridn(N_), kVB, 0, st_>>>(grid_, g, nvd, N_, sens_ + (size_t)c * N_,
                                                  eph_ + (size_t)l * N_, fhd_);
             T_TRY(cudaGetLastError());
