@@ -474,8 +474,9 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
 
 // Slow axis for the spectrum columns [blockIdx.x * W, +W) of every coil:
 // per s-parity a, forward FFT along s of x[s] w_2ns^{a s}, x Qf_l (parity a),
-// inverse FFT, times w_2ns^{-a s}; the two parities are summed in registers
-// and written back in place.  blockDim = W * R1: thread (w, j1).
+// inverse FFT, times w_2ns^{-a s}; the two parities are summed and written
+// back in place.  Both parities run at once as 2W tile columns (column a W + w
+// holds parity a of spectrum column w): blockDim = 2 W R1, thread (a, w, j1).
 constexpr int kSlowThreads = 256;
 
 // WC, NCOLC > 0: the block's column count W and the spectrum's column count
@@ -488,75 +489,76 @@ __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
     constexpr int LNS = ilog2c(NS);
     const int W = WC > 0 ? WC : W_rt;
     const int ncol = NCOLC > 0 ? NCOLC : ncol_rt;
-    extern __shared__ float2 E[];       // [NS][W] work
-    float2 *Y = E + NS * W;             // [NS][W] parity sum (each thread owns its slots)
+    extern __shared__ float2 E[];       // [NS][2W]
     if (done && *done) return;
     const int col0 = blockIdx.x * W;
     const int lw = WC > 0 ? ilog2c(WC) : __ffs(W) - 1;
-    const int w = threadIdx.x & (W - 1), j1 = threadIdx.x >> lw;
+    const int W2 = 2 * W, lw2 = lw + 1;
+    const int cw2 = threadIdx.x & (W2 - 1);  // tile column: a W + w
+    const int a = cw2 >> lw, w = cw2 & (W - 1);
+    const int j1 = threadIdx.x >> lw2;
     const size_t per_coil = (size_t)NS * ncol;
     for (int c = blockIdx.y; c < C; c += gridDim.y) {  // coils split over blockIdx.y
         float2 *bc = b1 + (size_t)c * per_coil + col0;
-        for (int a = 0; a < 2; ++a) {
-            {
-                float2 v[R2];
+        {   // stride pass, forward (both parities read the same column)
+            float2 v[R2];
 #pragma unroll
-                for (int q = 0; q < R2; ++q) {
-                    const int s = j1 + R1 * q;
-                    float2 xv = bc[(size_t)s * ncol + w];
-                    if (a) xv = cmul(xv, wn(tw, s, LNS + 1, false));
-                    v[q] = xv;
-                }
-                dft<R2, false>(v, tw);
-                if (j1 != 0) {
-#pragma unroll
-                    for (int q = 1; q < R2; ++q) v[q] = cmul(v[q], wn(tw, j1 * q, LNS, false));
-                }
-#pragma unroll
-                for (int q = 0; q < R2; ++q) E[(j1 + R1 * q) * W + w] = v[q];
+            for (int q = 0; q < R2; ++q) {
+                const int s = j1 + R1 * q;
+                float2 xv = bc[(size_t)s * ncol + w];
+                if (a) xv = cmul(xv, wn(tw, s, LNS + 1, false));
+                v[q] = xv;
             }
-            __syncthreads();
-            for (int it = threadIdx.x; it < W * R2; it += blockDim.x) {
-                const int w2 = it & (W - 1), k2 = it >> lw;
-                float2 z[R1];
+            dft<R2, false>(v, tw);
+            if (j1 != 0) {
 #pragma unroll
-                for (int k1 = 0; k1 < R1; ++k1) z[k1] = E[(k1 + R1 * k2) * W + w2];
-                dft<R1, false>(z, tw);
-#pragma unroll
-                for (int k1 = 0; k1 < R1; ++k1) {
-                    const int k = k2 + R2 * k1;
-                    z[k1] = cmul(z[k1], __ldg(&qf2[(size_t)(a * NS + k) * ncol + col0 + w2]));
-                }
-                dft<R1, true>(z, tw);
-                if (k2 != 0) {
-#pragma unroll
-                    for (int j = 1; j < R1; ++j) z[j] = cmul(z[j], wn(tw, j * k2, LNS, true));
-                }
-#pragma unroll
-                for (int j = 0; j < R1; ++j) E[(j + R1 * k2) * W + w2] = z[j];
+                for (int q = 1; q < R2; ++q) v[q] = cmul(v[q], wn(tw, j1 * q, LNS, false));
             }
-            __syncthreads();
-            {
-                float2 v[R2];
 #pragma unroll
-                for (int q = 0; q < R2; ++q) v[q] = E[(j1 + R1 * q) * W + w];
-                dft<R2, true>(v, tw);
-#pragma unroll
-                for (int q = 0; q < R2; ++q) {
-                    float2 xv = v[q];
-                    const int o = (j1 + R1 * q) * W + w;
-                    if (a) {
-                        xv = cmul(xv, wn(tw, j1 + R1 * q, LNS + 1, true));
-                        Y[o] = cadd(Y[o], xv);
-                    } else {
-                        Y[o] = xv;
-                    }
-                }
-            }
-            __syncthreads();
+            for (int q = 0; q < R2; ++q) E[(j1 + R1 * q) * W2 + cw2] = v[q];
         }
-#pragma unroll 4
-        for (int q = 0; q < R2; ++q) bc[(size_t)(j1 + R1 * q) * ncol + w] = Y[(j1 + R1 * q) * W + w];
+        __syncthreads();
+        // contiguous pass: forward, x Qf_l of the column's parity, inverse
+        for (int it = threadIdx.x; it < W2 * R2; it += blockDim.x) {
+            const int cw = it & (W2 - 1), k2 = it >> lw2;
+            const int aa = cw >> lw, ww = cw & (W - 1);
+            float2 z[R1];
+#pragma unroll
+            for (int k1 = 0; k1 < R1; ++k1) z[k1] = E[(k1 + R1 * k2) * W2 + cw];
+            dft<R1, false>(z, tw);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; ++k1) {
+                const int k = k2 + R2 * k1;
+                z[k1] = cmul(z[k1], __ldg(&qf2[(size_t)(aa * NS + k) * ncol + col0 + ww]));
+            }
+            dft<R1, true>(z, tw);
+            if (k2 != 0) {
+#pragma unroll
+                for (int j = 1; j < R1; ++j) z[j] = cmul(z[j], wn(tw, j * k2, LNS, true));
+            }
+#pragma unroll
+            for (int j = 0; j < R1; ++j) E[(j + R1 * k2) * W2 + cw] = z[j];
+        }
+        __syncthreads();
+        {   // stride pass, inverse, parity twiddle
+            float2 v[R2];
+#pragma unroll
+            for (int q = 0; q < R2; ++q) v[q] = E[(j1 + R1 * q) * W2 + cw2];
+            dft<R2, true>(v, tw);
+#pragma unroll
+            for (int q = 0; q < R2; ++q) {
+                float2 xv = v[q];
+                if (a) xv = cmul(xv, wn(tw, j1 + R1 * q, LNS + 1, true));
+                E[(j1 + R1 * q) * W2 + cw2] = xv;
+            }
+        }
+        __syncthreads();
+        // parity sum, written back in place (W consecutive columns per row)
+        for (int it = threadIdx.x; it < NS * W; it += blockDim.x) {
+            const int sidx = it >> lw, ww = it & (W - 1);
+            bc[(size_t)sidx * ncol + ww] = cadd(E[sidx * W2 + ww], E[sidx * W2 + W + ww]);
+        }
+        __syncthreads();  // the next coil rewrites the tile
     }
 }
 
@@ -620,7 +622,7 @@ cudaError_t set_slow_smem(size_t bytes) {
 // two specialised geometries (only when the plan's W and ncol are the ones
 // compiled in).
 int slow_spec(const ToepFftPlan &p) {
-    if (p.spec == 1 && p.ns == 256 && p.W == 16 && p.ncol == 32768) return 1;
+    if (p.spec == 1 && p.ns == 256 && p.W == 8 && p.ncol == 32768) return 1;
     if (p.spec == 2 && p.ns == 512 && p.W == 8 && p.ncol == 1024) return 2;
     return 0;
 }
@@ -669,7 +671,7 @@ bool toep_fft_plan(int ns, int nm, int nf, int C, ToepFftPlan *plan) {
     p.vpt = std::max(1, ecta / kPlaneThreads);
     p.ncol = p.qm * 2 * plane;
     const int r1 = split_r1(ns);
-    p.W = std::max(1, std::min(p.ncol, std::min(4096 / ns, kSlowThreads / r1)));
+    p.W = std::max(1, std::min(p.ncol, std::min(4096 / ns, kSlowThreads / (2 * r1))));
     p.smem_plane = (size_t)p.ps * nm * p.rs * sizeof(float2) + (size_t)ecta * sizeof(float2);
     p.smem_inv = p.smem_plane + (size_t)ecta * sizeof(float2);
     p.smem_slow = 2 * (size_t)ns * p.W * sizeof(float2);
@@ -709,7 +711,7 @@ bool toep_fft_plan(int ns, int nm, int nf, int C, ToepFftPlan *plan) {
         default: e = set_slow_smem<1024>(p.smem_slow); break;
     }
     if (e != cudaSuccess) return false;
-    if (slow_spec(p) == 1) e = set_slow_smem<256, 16, 32768>(p.smem_slow);
+    if (slow_spec(p) == 1) e = set_slow_smem<256, 8, 32768>(p.smem_slow);
     if (slow_spec(p) == 2) e = set_slow_smem<512, 8, 1024>(p.smem_slow);
     if (e != cudaSuccess) return false;
     *plan = p;
@@ -776,7 +778,7 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
                            ? p.C
                            : std::max(1, std::min(p.C, (2 * 148 + cols - 1) / cols));
     const dim3 blocks(cols, rows_y);
-    const int threads = p.W * r1;
+    const int threads = 2 * p.W * r1;
 #define IMP_SLOW_CASE(NSV)                                                                 \
     case NSV:                                                                              \
         k_slow<NSV><<<blocks, threads, p.smem_slow, st>>>(b1, qf2_l, p.C, p.ncol, p.W, tw, \
@@ -784,7 +786,7 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
         break;
     const int sspec = slow_spec(p);
     if (sspec == 1)
-        k_slow<256, 16, 32768><<<blocks, threads, p.smem_slow, st>>>(b1, qf2_l, p.C, p.ncol, p.W,
+        k_slow<256, 8, 32768><<<blocks, threads, p.smem_slow, st>>>(b1, qf2_l, p.C, p.ncol, p.W,
                                                                    tw, done);
     else if (sspec == 2)
         k_slow<512, 8, 1024><<<blocks, threads, p.smem_slow, st>>>(b1, qf2_l, p.C, p.ncol, p.W,
