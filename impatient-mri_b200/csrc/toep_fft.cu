@@ -234,12 +234,9 @@ struct PlaneGeoC {
     int ns, C;
 };
 
-// The compile-time-geometry instantiations keep the twiddle table in shared
-// memory (kTwN float2 after their regions); the generic ones read it through
-// the read-only global path.
-template <class Geo>
-constexpr bool kSmemTw = !std::is_same<Geo, PlaneGeo>::value;
-constexpr size_t kTwBytes = kTwN * sizeof(float2);
+// The compile-time-geometry kernels keep the twiddle table in shared memory
+// (kTwN float2 after their regions); the generic ones read it through the
+// read-only global path.
 
 // Shared-memory offset of element x of a row along f (skewed rows: x + x / r1f).
 template <class Geo>
@@ -254,11 +251,23 @@ __device__ __forceinline__ bool wait_bounded(uint64_t *bar, unsigned parity) {
     return false;
 }
 
+// Asynchronous 8-byte global -> shared copy (cp.async, L1-allocating), its
+// commit and the wait for all but the N most recent groups of this thread.
+__device__ __forceinline__ void cp_async8(float2 *dst, const float2 *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // Forward plane transform of coil c = blockIdx.y for the s-planes
-// [blockIdx.x * ps, +ps).  The padded input S_c e_l x is formed once in
-// shared memory (U); each (am, af) parity quadrant is then twiddled into the
-// work plane P, transformed, and written to b1[c][s][am][af][km][kf] in
-// natural frequency order.
+// [blockIdx.x * ps, +ps) (runtime geometry).  The padded input S_c e_l x is
+// formed once in shared memory (U); each (am, af) parity quadrant is then
+// twiddled into the work plane P, transformed, and written to
+// b1[c][s][am][af][km][kf] in natural frequency order.
 template <int VPT, class Geo = PlaneGeo>
 __global__ void __launch_bounds__(kPlaneThreads) k_fwd_plane(
     float2 *__restrict__ b1, const float2 *__restrict__ x, const float2 *__restrict__ sens,
@@ -267,11 +276,6 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fwd_plane(
     extern __shared__ float2 smem[];
     if (done && *done) return;
     const float2 *tw = tw_g;
-    if constexpr (kSmemTw<Geo>) {  // twiddle table after the plane regions
-        float2 *tws = smem + (size_t)g.ps * g.nm * g.rs + ((size_t)g.ps << g.lplane);
-        for (int i = threadIdx.x; i < kTwN; i += kPlaneThreads) tws[i] = __ldg(&tw_g[i]);
-        tw = tws;  // first read after the __syncthreads opening the quadrant loop
-    }
     const int plane = 1 << g.lplane;
     const int s0 = blockIdx.x * g.ps, c = blockIdx.y;
     const int ecta = g.ps << g.lplane;
@@ -335,6 +339,89 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fwd_plane(
         }
 }
 
+// Forward plane transform on a compile-time geometry, both f-parity quadrants
+// of an m-parity at once: the work planes P0 (af = 0) and P1 (af = 1) lie back
+// to back and their lines form one set, so each line pass has twice the items
+// (the one-pass rows of 32 and the stride pass of the rows of 512 otherwise
+// keep only half of the block's threads busy) and half as many barriers.  The
+// padded input S_c e_l x is kept in shared memory (U) only when both
+// m-parities read it (3-D); 2-D blocks form it on the fly.
+template <class Geo>
+__global__ void __launch_bounds__(kPlaneThreads) k_fwd_pair(
+    float2 *__restrict__ b1, const float2 *__restrict__ x, const float2 *__restrict__ sens,
+    const float2 *__restrict__ eph_l, Geo g, const float2 *__restrict__ tw_g,
+    const int *__restrict__ done) {
+    constexpr int plane = 1 << Geo::lplane, ecta = Geo::ps * plane;
+    constexpr int VPT = ecta / kPlaneThreads;
+    constexpr int pstride = Geo::nm * Geo::rs, par = Geo::ps * pstride;
+    constexpr bool kU = Geo::qm == 2;
+    static_assert(ecta % kPlaneThreads == 0, "whole elements per thread");
+    extern __shared__ float2 smem[];
+    if (done && *done) return;
+    float2 *P = smem;                     // [af][ps][nm][rs]
+    float2 *U = smem + 2 * par;           // [ps][plane], kU only
+    float2 *tw = U + (kU ? ecta : 0);     // twiddle table
+    for (int i = threadIdx.x; i < kTwN; i += kPlaneThreads) tw[i] = __ldg(&tw_g[i]);
+    const int s0 = blockIdx.x * Geo::ps, c = blockIdx.y;
+    const size_t N = (size_t)g.ns << Geo::lplane;
+    const size_t vbase = (size_t)s0 << Geo::lplane;
+    const Lines rows{Geo::lps + Geo::lnm + 1, Geo::lps + Geo::lnm + 1, Geo::rs, 0, 1, Geo::sk};
+    const Lines cols{Geo::lps + Geo::lnf + 1, Geo::lnf, 1, pstride, Geo::rs};
+    const float2 *sc = sens + (size_t)c * N + vbase;
+    const float2 *ec = eph_l + vbase;
+    const float2 *xc = x + vbase;
+    if constexpr (kU) {
+#pragma unroll
+        for (int i = 0; i < VPT; ++i) {
+            const int e = threadIdx.x + i * kPlaneThreads;  // read back by this thread only
+            U[e] = cmul(cmul(__ldg(&sc[e]), __ldg(&ec[e])), __ldg(&xc[e]));
+        }
+    }
+    for (int am = 0; am < Geo::qm; ++am) {
+        __syncthreads();  // twiddle table loaded / previous outputs read
+#pragma unroll
+        for (int i = 0; i < VPT; ++i) {
+            const int e = threadIdx.x + i * kPlaneThreads;
+            const int pp = e >> Geo::lplane, r = e & (plane - 1);
+            const int m = r >> Geo::lnf, f = r & (Geo::nf - 1);
+            float2 val;
+            if constexpr (kU) val = U[e];
+            else val = cmul(cmul(__ldg(&sc[e]), __ldg(&ec[e])), __ldg(&xc[e]));
+            if (am) val = cmul(val, wn(tw, m, Geo::lnm + 1, false));
+            const int o = pp * pstride + m * Geo::rs + fphys(g, f);
+            P[o] = val;
+            P[par + o] = cmul(val, wn(tw, f, Geo::lnf + 1, false));
+        }
+        __syncthreads();
+        run_stride<false>(P, rows, Geo::r1f, Geo::r2f, Geo::lnf, true, tw);
+        __syncthreads();
+        if constexpr (Geo::r1f > 1) {
+            run_contig<false>(P, rows, Geo::r1f, Geo::r2f, Geo::lnf, tw);
+            __syncthreads();
+        }
+        if constexpr (Geo::nm > 1) {
+            run_stride<false>(P, cols, Geo::r1m, Geo::r2m, Geo::lnm, true, tw);
+            __syncthreads();
+            if constexpr (Geo::r1m > 1) {
+                run_contig<false>(P, cols, Geo::r1m, Geo::r2m, Geo::lnm, tw);
+                __syncthreads();
+            }
+        }
+        float2 *dst = b1 + ((size_t)c * g.ns + s0) * Geo::ncol + ((size_t)(am * 2) << Geo::lplane);
+#pragma unroll
+        for (int i = 0; i < VPT; ++i) {
+            const int e = threadIdx.x + i * kPlaneThreads;
+            const int pp = e >> Geo::lplane, r = e & (plane - 1);
+            const int km = r >> Geo::lnf, kf = r & (Geo::nf - 1);
+            const int sm = Geo::nm > 1 ? slot_of(km, Geo::r1m, Geo::lr2m) : 0;
+            const int o = pp * pstride + sm * Geo::rs + fphys(g, slot_of(kf, Geo::r1f, Geo::lr2f));
+            float2 *d = dst + (size_t)pp * Geo::ncol + r;
+            d[0] = P[o];
+            d[plane] = P[par + o];
+        }
+    }
+}
+
 // Inverse plane transform for the s-planes [blockIdx.x * ps, +ps).  The
 // blockDim.y-wide cluster (cluster rank = blockIdx.y) splits the coils: block
 // r takes coils r, r + csize, ...  Each parity quadrant of b1 is brought into
@@ -364,14 +451,6 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
     const int rank = blockIdx.y, csize = gridDim.y;
     const int s0 = blockIdx.x * g.ps;
     const float2 *tw = tw_g;
-    if constexpr (kSmemTw<Geo>) {  // twiddle table after the three regions
-        if (!skip) {
-            float2 *tws = smem + 2 * (size_t)ecta + (size_t)g.ps * pstride;
-            for (int i = threadIdx.x; i < kTwN; i += kPlaneThreads) tws[i] = __ldg(&tw_g[i]);
-            __syncthreads();
-            tw = tws;
-        }
-    }
     if (!skip) {
         const size_t N = (size_t)g.ns << g.lplane;
         const size_t vbase = (size_t)s0 << g.lplane;
@@ -470,6 +549,121 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
         }
     }
     cluster.sync();  // no block leaves while another still reads its Y
+}
+
+// Inverse plane transform on a compile-time geometry (same work split and
+// result as k_inv_plane).  Each parity quadrant of b1 is copied straight into
+// a work plane in slot order by per-thread 8-byte cp.async copies (coalesced:
+// a warp reads 32 consecutive spectrum values), two work planes alternating so
+// that the next quadrant's copies land while this one is transformed; no
+// staging buffer and no scatter pass.  Each thread keeps the partial coil sum
+// of its own elements in registers; after the last quadrant the sums go to
+// shared memory (over the work planes) for the cluster's coil reduction.
+template <class Geo>
+__global__ void __launch_bounds__(kPlaneThreads) k_inv_async(
+    float2 *__restrict__ q, const float2 *__restrict__ b1, const float2 *__restrict__ sens,
+    const float2 *__restrict__ eph_l, Geo g, int first, const float2 *__restrict__ tw_g,
+    const int *__restrict__ done) {
+    constexpr int plane = 1 << Geo::lplane, ecta = Geo::ps * plane;
+    constexpr int VPT = ecta / kPlaneThreads;
+    constexpr int pstride = Geo::nm * Geo::rs, buf = Geo::ps * pstride;
+    constexpr int nquad = Geo::qm * 2;
+    static_assert(ecta % kPlaneThreads == 0 && ecta <= 2 * buf, "plane split / partial sums");
+    extern __shared__ __align__(16) float2 smem[];
+    cg::cluster_group cluster = cg::this_cluster();
+    float2 *tw = smem + 2 * buf;
+    float2 *Y = smem;  // partial coil sums, after the last transform
+    const bool skip = done && *done;
+    const int rank = blockIdx.y, csize = gridDim.y;
+    const int s0 = blockIdx.x * Geo::ps;
+    const size_t N = (size_t)g.ns << Geo::lplane;
+    const size_t vbase = (size_t)s0 << Geo::lplane;
+    float2 y[VPT];
+#pragma unroll
+    for (int i = 0; i < VPT; ++i) y[i] = make_float2(0.f, 0.f);
+    if (!skip) {
+        for (int i = threadIdx.x; i < kTwN; i += kPlaneThreads) tw[i] = __ldg(&tw_g[i]);
+        const Lines rows{Geo::lps + Geo::lnm, Geo::lps + Geo::lnm, Geo::rs, 0, 1, Geo::sk};
+        const Lines cols{Geo::lps + Geo::lnf, Geo::lnf, 1, pstride, Geo::rs};
+        const int my_coils = (g.C - rank + csize - 1) / csize;
+        const int nq = my_coils * nquad;
+        auto issue = [&](int qi) {
+            const int c = rank + (qi / nquad) * csize, quad = qi % nquad;
+            const float2 *src = b1 + ((size_t)c * g.ns + s0) * Geo::ncol + ((size_t)quad << Geo::lplane);
+            float2 *P = smem + (qi & 1) * buf;
+#pragma unroll
+            for (int i = 0; i < VPT; ++i) {
+                const int e = threadIdx.x + i * kPlaneThreads;
+                const int pp = e >> Geo::lplane, r = e & (plane - 1);
+                const int km = r >> Geo::lnf, kf = r & (Geo::nf - 1);
+                const int sm = Geo::nm > 1 ? slot_of(km, Geo::r1m, Geo::lr2m) : 0;
+                cp_async8(P + pp * pstride + sm * Geo::rs + fphys(g, slot_of(kf, Geo::r1f, Geo::lr2f)),
+                          src + (size_t)pp * Geo::ncol + r);
+            }
+            cp_async_commit();
+        };
+        if (nq > 0) issue(0);
+        for (int qi = 0; qi < nq; ++qi) {
+            __syncthreads();  // every thread is done with the plane the next copy overwrites
+            if (qi + 1 < nq) {
+                issue(qi + 1);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();  // quadrant qi (and the twiddle table) visible to all threads
+            float2 *P = smem + (qi & 1) * buf;
+            const int c = rank + (qi / nquad) * csize, quad = qi % nquad;
+            const int am = quad >> 1, af = quad & 1;
+            if constexpr (Geo::nm > 1) {
+                if constexpr (Geo::r1m > 1) {
+                    run_contig<true>(P, cols, Geo::r1m, Geo::r2m, Geo::lnm, tw);
+                    __syncthreads();
+                }
+                run_stride<true>(P, cols, Geo::r1m, Geo::r2m, Geo::lnm, false, tw);
+                __syncthreads();
+            }
+            if constexpr (Geo::r1f > 1) {
+                run_contig<true>(P, rows, Geo::r1f, Geo::r2f, Geo::lnf, tw);
+                __syncthreads();
+            }
+            run_stride<true>(P, rows, Geo::r1f, Geo::r2f, Geo::lnf, false, tw);
+            __syncthreads();
+            const float2 *sc = sens + (size_t)c * N + vbase;
+#pragma unroll
+            for (int i = 0; i < VPT; ++i) {
+                const int e = threadIdx.x + i * kPlaneThreads;
+                const int pp = e >> Geo::lplane, r = e & (plane - 1);
+                const int m = r >> Geo::lnf, f = r & (Geo::nf - 1);
+                float2 val = P[pp * pstride + m * Geo::rs + fphys(g, f)];
+                if (am) val = cmul(val, wn(tw, m, Geo::lnm + 1, true));
+                if (af) val = cmul(val, wn(tw, f, Geo::lnf + 1, true));
+                y[i] = cadd(y[i], cmulc(__ldg(&sc[e]), val));
+            }
+        }
+        __syncthreads();  // the work planes become the partial-sum array
+#pragma unroll
+        for (int i = 0; i < VPT; ++i) Y[threadIdx.x + i * kPlaneThreads] = y[i];
+    }
+    cluster.sync();
+    if (!skip) {
+        const int share = (ecta + csize - 1) / csize;
+        const int e0 = rank * share, e1 = min(ecta, e0 + share);
+        for (int e = e0 + threadIdx.x; e < e1; e += kPlaneThreads) {
+            float2 sum = make_float2(0.f, 0.f);
+            for (int r = 0; r < csize; ++r) sum = cadd(sum, cluster.map_shared_rank(Y, r)[e]);
+            const size_t v = vbase + e;
+            float2 out = cmulc(eph_l[v], sum);
+            if (!first) out = cadd(out, q[v]);
+            q[v] = out;
+        }
+    }
+    cluster.sync();  // no block leaves while another still reads its Y
+}
+
+template <class Geo>
+constexpr size_t inv_async_smem() {  // k_inv_async: two work planes, twiddle table
+    return ((size_t)2 * Geo::ps * Geo::nm * Geo::rs + kTwN) * sizeof(float2);
 }
 
 // Slow axis for the spectrum columns [blockIdx.x * W, +W) of every coil:
@@ -582,13 +776,28 @@ __global__ void k_qf_perm(float2 *__restrict__ qf2, const float2 *__restrict__ q
 
 bool pow2(int n) { return n >= 1 && (n & (n - 1)) == 0; }
 
+template <class Geo>
+constexpr size_t pair_smem() {  // k_fwd_pair: P0, P1, U (3-D), twiddle table
+    return ((size_t)2 * Geo::ps * Geo::nm * Geo::rs + (Geo::qm == 2 ? (size_t)Geo::ps << Geo::lplane : 0) +
+            kTwN) * sizeof(float2);
+}
+
 template <int VPT, class Geo = PlaneGeo>
 cudaError_t set_plane_smem(size_t fwd_bytes, size_t inv_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(
-        k_fwd_plane<VPT, Geo>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fwd_bytes);
+    cudaError_t e;
+    if constexpr (std::is_same<Geo, PlaneGeo>::value)
+        e = cudaFuncSetAttribute(k_fwd_plane<VPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)fwd_bytes);
+    else
+        e = cudaFuncSetAttribute(k_fwd_pair<Geo>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)pair_smem<Geo>());
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_inv_plane<VPT, Geo>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_bytes);
+    if constexpr (std::is_same<Geo, PlaneGeo>::value)
+        return cudaFuncSetAttribute(k_inv_plane<VPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)inv_bytes);
+    else
+        return cudaFuncSetAttribute(k_inv_async<Geo>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)inv_async_smem<Geo>());
 }
 
 // Plane geometries with compile-time instantiations: 3-D 256 x 256 x 32 images
@@ -596,6 +805,9 @@ cudaError_t set_plane_smem(size_t fwd_bytes, size_t inv_bytes) {
 // 16 per block).  Others run the generic (runtime-geometry) kernels.
 using GeoC3d = PlaneGeoC<256, 32, 1>;
 using GeoC2d = PlaneGeoC<1, 512, 16>;
+static_assert(pair_smem<GeoC3d>() <= 227 * 1024 && pair_smem<GeoC2d>() <= 227 * 1024 &&
+                  inv_async_smem<GeoC3d>() <= 227 * 1024 && inv_async_smem<GeoC2d>() <= 227 * 1024,
+              "shared memory of the compile-time-geometry plane kernels");
 // IMP_TOEP_GENERIC=1 keeps the generic kernels (the tests compare both).
 int spec_kind(const ToepFftPlan &p) {
     const char *gen = std::getenv("IMP_TOEP_GENERIC");
@@ -694,9 +906,8 @@ bool toep_fft_plan(int ns, int nm, int nf, int C, ToepFftPlan *plan) {
     }
     if (e != cudaSuccess) return false;
     p.spec = spec_kind(p);
-    if (p.smem_inv + kTwBytes > kMaxSmem) p.spec = 0;  // no room for the twiddle table
-    if (p.spec == 1) e = set_plane_smem<16, GeoC3d>(p.smem_plane + kTwBytes, p.smem_inv + kTwBytes);
-    if (p.spec == 2) e = set_plane_smem<16, GeoC2d>(p.smem_plane + kTwBytes, p.smem_inv + kTwBytes);
+    if (p.spec == 1) e = set_plane_smem<16, GeoC3d>(0, 0);
+    if (p.spec == 2) e = set_plane_smem<16, GeoC2d>(0, 0);
     if (e != cudaSuccess) return false;
     switch (ns) {
         case 2: e = set_slow_smem<2>(p.smem_slow); break;
@@ -750,10 +961,10 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
                                                                 done);                      \
         break;
     if (spec == 1) {
-        k_fwd_plane<16, GeoC3d><<<ga, kPlaneThreads, p.smem_plane + kTwBytes, st>>>(
+        k_fwd_pair<GeoC3d><<<ga, kPlaneThreads, pair_smem<GeoC3d>(), st>>>(
             b1, x, sens, eph_l, geo_c<GeoC3d>(p), tw, done);
     } else if (spec == 2) {
-        k_fwd_plane<16, GeoC2d><<<ga, kPlaneThreads, p.smem_plane + kTwBytes, st>>>(
+        k_fwd_pair<GeoC2d><<<ga, kPlaneThreads, pair_smem<GeoC2d>(), st>>>(
             b1, x, sens, eph_l, geo_c<GeoC2d>(p), tw, done);
     } else {
         switch (p.vpt) {
@@ -808,7 +1019,9 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(p.ns / p.ps, p.csize);
     cfg.blockDim = dim3(kPlaneThreads);
-    cfg.dynamicSmemBytes = p.smem_inv + (spec ? kTwBytes : 0);
+    cfg.dynamicSmemBytes = spec == 1   ? inv_async_smem<GeoC3d>()
+                           : spec == 2 ? inv_async_smem<GeoC2d>()
+                                       : p.smem_inv;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -819,11 +1032,11 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
     cfg.numAttrs = 1;
     cudaError_t e;
     if (spec == 1)
-        e = cudaLaunchKernelEx(&cfg, k_inv_plane<16, GeoC3d>, q, b1, sens, eph_l,
-                               geo_c<GeoC3d>(p), first, tw, done, err);
+        e = cudaLaunchKernelEx(&cfg, k_inv_async<GeoC3d>, q, b1, sens, eph_l, geo_c<GeoC3d>(p),
+                               first, tw, done);
     else if (spec == 2)
-        e = cudaLaunchKernelEx(&cfg, k_inv_plane<16, GeoC2d>, q, b1, sens, eph_l,
-                               geo_c<GeoC2d>(p), first, tw, done, err);
+        e = cudaLaunchKernelEx(&cfg, k_inv_async<GeoC2d>, q, b1, sens, eph_l, geo_c<GeoC2d>(p),
+                               first, tw, done);
     else switch (p.vpt) {
         case 1: e = cudaLaunchKernelEx(&cfg, k_inv_plane<1>, q, b1, sens, eph_l, g, first, tw, done, err); break;
         case 2: e = cudaLaunchKernelEx(&cfg, k_inv_plane<2>, q, b1, sens, eph_l, g, first, tw, done, err); break;
