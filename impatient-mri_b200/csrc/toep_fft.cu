@@ -251,10 +251,15 @@ __device__ __forceinline__ bool wait_bounded(uint64_t *bar, unsigned parity) {
     return false;
 }
 
-// Asynchronous 8-byte global -> shared copy (cp.async, L1-allocating), its
-// commit and the wait for all but the N most recent groups of this thread.
+// Asynchronous global -> shared copies (cp.async: 8 bytes L1-allocating, 16
+// bytes L2 only), their commit and the wait for all but the N most recent
+// groups of this thread.
 __device__ __forceinline__ void cp_async8(float2 *dst, const float2 *src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16(float2 *dst, const float2 *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src)
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
@@ -377,20 +382,26 @@ __global__ void __launch_bounds__(kPlaneThreads) k_fwd_pair(
             U[e] = cmul(cmul(__ldg(&sc[e]), __ldg(&ec[e])), __ldg(&xc[e]));
         }
     }
+    // f = e mod nf is the same for all of a thread's elements (nf divides the
+    // block size): one f-parity twiddle per thread, read once.
+    static_assert(kPlaneThreads % Geo::nf == 0, "f fixed per thread");
+    const int fth = threadIdx.x & (Geo::nf - 1);
+    float2 wf = make_float2(1.f, 0.f);
     for (int am = 0; am < Geo::qm; ++am) {
         __syncthreads();  // twiddle table loaded / previous outputs read
+        if (am == 0) wf = wn(tw, fth, Geo::lnf + 1, false);
 #pragma unroll
         for (int i = 0; i < VPT; ++i) {
             const int e = threadIdx.x + i * kPlaneThreads;
             const int pp = e >> Geo::lplane, r = e & (plane - 1);
-            const int m = r >> Geo::lnf, f = r & (Geo::nf - 1);
+            const int m = r >> Geo::lnf;
             float2 val;
             if constexpr (kU) val = U[e];
             else val = cmul(cmul(__ldg(&sc[e]), __ldg(&ec[e])), __ldg(&xc[e]));
             if (am) val = cmul(val, wn(tw, m, Geo::lnm + 1, false));
-            const int o = pp * pstride + m * Geo::rs + fphys(g, f);
+            const int o = pp * pstride + m * Geo::rs + fphys(g, fth);
             P[o] = val;
-            P[par + o] = cmul(val, wn(tw, f, Geo::lnf + 1, false));
+            P[par + o] = cmul(val, wf);
         }
         __syncthreads();
         run_stride<false>(P, rows, Geo::r1f, Geo::r2f, Geo::lnf, true, tw);
@@ -573,11 +584,13 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_async(
     cg::cluster_group cluster = cg::this_cluster();
     float2 *tw = smem + 2 * buf;
     float2 *Y = smem;  // partial coil sums, after the last transform
+    static_assert(kPlaneThreads % Geo::nf == 0, "f fixed per thread");
     const bool skip = done && *done;
     const int rank = blockIdx.y, csize = gridDim.y;
     const int s0 = blockIdx.x * Geo::ps;
     const size_t N = (size_t)g.ns << Geo::lplane;
     const size_t vbase = (size_t)s0 << Geo::lplane;
+    const int fth = threadIdx.x & (Geo::nf - 1);  // f of every element of this thread
     float2 y[VPT];
 #pragma unroll
     for (int i = 0; i < VPT; ++i) y[i] = make_float2(0.f, 0.f);
@@ -630,14 +643,15 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_async(
             run_stride<true>(P, rows, Geo::r1f, Geo::r2f, Geo::lnf, false, tw);
             __syncthreads();
             const float2 *sc = sens + (size_t)c * N + vbase;
+            const float2 wf = wn(tw, fth, Geo::lnf + 1, true);
 #pragma unroll
             for (int i = 0; i < VPT; ++i) {
                 const int e = threadIdx.x + i * kPlaneThreads;
                 const int pp = e >> Geo::lplane, r = e & (plane - 1);
-                const int m = r >> Geo::lnf, f = r & (Geo::nf - 1);
-                float2 val = P[pp * pstride + m * Geo::rs + fphys(g, f)];
+                const int m = r >> Geo::lnf;
+                float2 val = P[pp * pstride + m * Geo::rs + fphys(g, fth)];
                 if (am) val = cmul(val, wn(tw, m, Geo::lnm + 1, true));
-                if (af) val = cmul(val, wn(tw, f, Geo::lnf + 1, true));
+                if (af) val = cmul(val, wf);
                 y[i] = cadd(y[i], cmulc(__ldg(&sc[e]), val));
             }
         }
@@ -671,20 +685,42 @@ constexpr size_t inv_async_smem() {  // k_inv_async: two work planes, twiddle ta
 // inverse FFT, times w_2ns^{-a s}; the two parities are summed and written
 // back in place.  Both parities run at once as 2W tile columns (column a W + w
 // holds parity a of spectrum column w): blockDim = 2 W R1, thread (a, w, j1).
+// TWS: the twiddle table sits in shared memory after the tile (else it is read
+// through the read-only global path; the 2-D 512-row instantiation, whose two
+// blocks per SM keep more L1 that way, measures faster so).  STAGE (blocks that
+// loop over several coils): the block's Qf_l columns are copied into shared
+// memory once (cp.async) and read from there by every coil, and the next
+// coil's input columns are copied in while the current coil is transformed.
 constexpr int kSlowThreads = 256;
+
+template <int NS, int W>
+struct SlowStage {  // shared-memory layout of the STAGE kernels (float2 offsets)
+    static constexpr int tile = 2 * NS * W;           // E [NS][2W]
+    static constexpr int qpar = NS * W + 8;           // Qs parity stride (8: other bank half)
+    static constexpr int qs = tile + kTwN;            // Qs [2][NS][W] (+pad)
+    static constexpr int xs = qs + 2 * qpar;          // Xs [NS][W]
+    static constexpr int total = xs + NS * W;
+};
 
 // WC, NCOLC > 0: the block's column count W and the spectrum's column count
 // ncol as compile-time constants (the runtime arguments are then ignored).
-template <int NS, int WC = 0, int NCOLC = 0>
+template <int NS, int WC = 0, int NCOLC = 0, bool STAGE = false, bool TWS = true>
 __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
     float2 *__restrict__ b1, const float2 *__restrict__ qf2, int C, int ncol_rt, int W_rt,
-    const float2 *__restrict__ tw, const int *__restrict__ done) {
+    const float2 *__restrict__ tw_g, const int *__restrict__ done) {
     constexpr int R1 = split_r1(NS), R2 = NS / R1;
     constexpr int LNS = ilog2c(NS);
+    static_assert(!STAGE || (WC > 0 && WC % 2 == 0 && NCOLC > 0 && TWS), "staged tiles: 16-byte rows");
     const int W = WC > 0 ? WC : W_rt;
     const int ncol = NCOLC > 0 ? NCOLC : ncol_rt;
-    extern __shared__ float2 E[];       // [NS][2W]
+    extern __shared__ __align__(16) float2 E[];       // [NS][2W], twiddle table, staging
     if (done && *done) return;
+    const float2 *tw = tw_g;
+    if constexpr (TWS) {
+        float2 *tws = E + 2 * NS * W;
+        for (int i = threadIdx.x; i < kTwN; i += blockDim.x) tws[i] = __ldg(&tw_g[i]);
+        tw = tws;
+    }
     const int col0 = blockIdx.x * W;
     const int lw = WC > 0 ? ilog2c(WC) : __ffs(W) - 1;
     const int W2 = 2 * W, lw2 = lw + 1;
@@ -692,14 +728,41 @@ __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
     const int a = cw2 >> lw, w = cw2 & (W - 1);
     const int j1 = threadIdx.x >> lw2;
     const size_t per_coil = (size_t)NS * ncol;
-    for (int c = blockIdx.y; c < C; c += gridDim.y) {  // coils split over blockIdx.y
+    float2 *Qs = nullptr, *Xs = nullptr;
+    if constexpr (STAGE) {
+        Qs = E + SlowStage<NS, WC>::qs;
+        Xs = E + SlowStage<NS, WC>::xs;
+    }
+    // STAGE: rows of W float2 as W / 2 16-byte pieces
+    auto stage_x = [&](int c) {
+        const float2 *src = b1 + (size_t)c * per_coil + col0;
+        for (int i = threadIdx.x; i < NS * (W / 2); i += blockDim.x) {
+            const int row = i / (W / 2), pc = 2 * (i % (W / 2));
+            cp_async16(Xs + row * W + pc, src + (size_t)row * ncol + pc);
+        }
+        cp_async_commit();
+    };
+    if constexpr (STAGE) {
+        for (int i = threadIdx.x; i < 2 * NS * (W / 2); i += blockDim.x) {
+            const int row = i / (W / 2), pc = 2 * (i % (W / 2));
+            const int aa = row / NS, k = row % NS;
+            cp_async16(Qs + aa * SlowStage<NS, WC>::qpar + k * W + pc,
+                       qf2 + (size_t)row * ncol + col0 + pc);
+        }
+        stage_x(blockIdx.y);  // one group: Qf columns and the first coil's input
+    }
+    for (int c = blockIdx.y; c < C; c += gridDim.y) {
         float2 *bc = b1 + (size_t)c * per_coil + col0;
+        if constexpr (STAGE) cp_async_wait<0>();
+        __syncthreads();  // twiddle table / staged tiles visible; previous coil's tile reads done
         {   // stride pass, forward (both parities read the same column)
             float2 v[R2];
 #pragma unroll
             for (int q = 0; q < R2; ++q) {
                 const int s = j1 + R1 * q;
-                float2 xv = bc[(size_t)s * ncol + w];
+                float2 xv;
+                if constexpr (STAGE) xv = Xs[s * W + w];
+                else xv = bc[(size_t)s * ncol + w];
                 if (a) xv = cmul(xv, wn(tw, s, LNS + 1, false));
                 v[q] = xv;
             }
@@ -712,6 +775,9 @@ __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
             for (int q = 0; q < R2; ++q) E[(j1 + R1 * q) * W2 + cw2] = v[q];
         }
         __syncthreads();
+        if constexpr (STAGE) {
+            if (c + (int)gridDim.y < C) stage_x(c + gridDim.y);  // lands during this coil's work
+        }
         // contiguous pass: forward, x Qf_l of the column's parity, inverse
         for (int it = threadIdx.x; it < W2 * R2; it += blockDim.x) {
             const int cw = it & (W2 - 1), k2 = it >> lw2;
@@ -723,7 +789,10 @@ __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
 #pragma unroll
             for (int k1 = 0; k1 < R1; ++k1) {
                 const int k = k2 + R2 * k1;
-                z[k1] = cmul(z[k1], __ldg(&qf2[(size_t)(aa * NS + k) * ncol + col0 + ww]));
+                float2 qv;
+                if constexpr (STAGE) qv = Qs[aa * SlowStage<NS, WC>::qpar + k * W + ww];
+                else qv = __ldg(&qf2[(size_t)(aa * NS + k) * ncol + col0 + ww]);
+                z[k1] = cmul(z[k1], qv);
             }
             dft<R1, true>(z, tw);
             if (k2 != 0) {
@@ -752,8 +821,13 @@ __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
             const int sidx = it >> lw, ww = it & (W - 1);
             bc[(size_t)sidx * ncol + ww] = cadd(E[sidx * W2 + ww], E[sidx * W2 + W + ww]);
         }
-        __syncthreads();  // the next coil rewrites the tile
     }
+}
+
+template <int NS, int WC = 0, int NCOLC = 0, bool STAGE = false, bool TWS = true>
+size_t slow_smem(int W) {  // dynamic shared memory of k_slow
+    if constexpr (STAGE) return (size_t)SlowStage<NS, WC>::total * sizeof(float2);
+    return ((size_t)2 * NS * W + (TWS ? kTwN : 0)) * sizeof(float2);
 }
 
 __global__ void k_qf_perm(float2 *__restrict__ qf2, const float2 *__restrict__ qf, int ns, int nm,
@@ -824,10 +898,11 @@ G geo_c(const ToepFftPlan &p) {
     return g;
 }
 
-template <int NS, int WC = 0, int NCOLC = 0>
-cudaError_t set_slow_smem(size_t bytes) {
-    return cudaFuncSetAttribute(k_slow<NS, WC, NCOLC>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+template <int NS, int WC = 0, int NCOLC = 0, bool STAGE = false, bool TWS = true>
+cudaError_t set_slow_smem(int W) {
+    return cudaFuncSetAttribute(k_slow<NS, WC, NCOLC, STAGE, TWS>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)slow_smem<NS, WC, NCOLC, STAGE, TWS>(W));
 }
 
 // Slow-axis instantiations with compile-time block and spectrum widths for the
@@ -886,7 +961,7 @@ bool toep_fft_plan(int ns, int nm, int nf, int C, ToepFftPlan *plan) {
     p.W = std::max(1, std::min(p.ncol, std::min(4096 / ns, kSlowThreads / (2 * r1))));
     p.smem_plane = (size_t)p.ps * nm * p.rs * sizeof(float2) + (size_t)ecta * sizeof(float2);
     p.smem_inv = p.smem_plane + (size_t)ecta * sizeof(float2);
-    p.smem_slow = 2 * (size_t)ns * p.W * sizeof(float2);
+    p.smem_slow = ((size_t)2 * ns * p.W + kTwN) * sizeof(float2);
     constexpr size_t kMaxSmem = 227 * 1024 - 64;  // room for the static mbarrier
     if (p.smem_inv > kMaxSmem || p.smem_slow > kMaxSmem) return false;
     for (int cs = std::min(C, 8); cs >= 1; --cs)
@@ -910,20 +985,23 @@ bool toep_fft_plan(int ns, int nm, int nf, int C, ToepFftPlan *plan) {
     if (p.spec == 2) e = set_plane_smem<16, GeoC2d>(0, 0);
     if (e != cudaSuccess) return false;
     switch (ns) {
-        case 2: e = set_slow_smem<2>(p.smem_slow); break;
-        case 4: e = set_slow_smem<4>(p.smem_slow); break;
-        case 8: e = set_slow_smem<8>(p.smem_slow); break;
-        case 16: e = set_slow_smem<16>(p.smem_slow); break;
-        case 32: e = set_slow_smem<32>(p.smem_slow); break;
-        case 64: e = set_slow_smem<64>(p.smem_slow); break;
-        case 128: e = set_slow_smem<128>(p.smem_slow); break;
-        case 256: e = set_slow_smem<256>(p.smem_slow); break;
-        case 512: e = set_slow_smem<512>(p.smem_slow); break;
-        default: e = set_slow_smem<1024>(p.smem_slow); break;
+        case 2: e = set_slow_smem<2>(p.W); break;
+        case 4: e = set_slow_smem<4>(p.W); break;
+        case 8: e = set_slow_smem<8>(p.W); break;
+        case 16: e = set_slow_smem<16>(p.W); break;
+        case 32: e = set_slow_smem<32>(p.W); break;
+        case 64: e = set_slow_smem<64>(p.W); break;
+        case 128: e = set_slow_smem<128>(p.W); break;
+        case 256: e = set_slow_smem<256>(p.W); break;
+        case 512: e = set_slow_smem<512>(p.W); break;
+        default: e = set_slow_smem<1024>(p.W); break;
     }
     if (e != cudaSuccess) return false;
-    if (slow_spec(p) == 1) e = set_slow_smem<256, 8, 32768>(p.smem_slow);
-    if (slow_spec(p) == 2) e = set_slow_smem<512, 8, 1024>(p.smem_slow);
+    if (slow_spec(p) == 1) {
+        e = set_slow_smem<256, 8, 32768>(p.W);
+        if (e == cudaSuccess) e = set_slow_smem<256, 8, 32768, true>(p.W);
+    }
+    if (slow_spec(p) == 2) e = set_slow_smem<512, 8, 1024, false, false>(p.W);
     if (e != cudaSuccess) return false;
     *plan = p;
     return true;
@@ -996,12 +1074,16 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
                                                           done);                           \
         break;
     const int sspec = slow_spec(p);
-    if (sspec == 1)
+    if (sspec == 1 && rows_y < p.C)
+        k_slow<256, 8, 32768, true><<<blocks, threads, slow_smem<256, 8, 32768, true>(p.W), st>>>(
+            b1, qf2_l, p.C, p.ncol, p.W, tw, done);
+    else if (sspec == 1)
         k_slow<256, 8, 32768><<<blocks, threads, p.smem_slow, st>>>(b1, qf2_l, p.C, p.ncol, p.W,
                                                                    tw, done);
     else if (sspec == 2)
-        k_slow<512, 8, 1024><<<blocks, threads, p.smem_slow, st>>>(b1, qf2_l, p.C, p.ncol, p.W,
-                                                                 tw, done);
+        k_slow<512, 8, 1024, false, false>
+            <<<blocks, threads, slow_smem<512, 8, 1024, false, false>(p.W), st>>>(
+                b1, qf2_l, p.C, p.ncol, p.W, tw, done);
     else switch (p.ns) {
         IMP_SLOW_CASE(2)
         IMP_SLOW_CASE(4)
