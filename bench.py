@@ -837,9 +837,13 @@ def run_toeplitz(args, ws, rank, local):
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
-                     "kernel": "A^H A application inside the CG (pruned FFT engine: k_fwd_plane, "
-                               "k_slow with x Qf_l, k_inv_plane with the coil sum; CG update), "
+                     "frac": achieved / hbm,
+                     "traffic": ncu_traffic("toeplitz_apply_toep3d_256x256x32.md",
+                                            "traffic_bytes_per_apply:"),
+                     "traffic_source": "profiles/toeplitz_apply_toep3d_256x256x32.md: DRAM bytes "
+                                       "of the three engine kernels of one application (ncu)",
+                     "kernel": "A^H A application inside the CG (pruned FFT engine: k_fwd_pair, "
+                               "k_slow with x Qf_l, k_inv_async with the coil sum; CG update), "
                                "per application; bytes = the zero-padded FFT model",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback",
                      "algorithmic_bytes_per_apply": model, "apply_ms": per_apply_s * 1e3,
@@ -1231,8 +1235,8 @@ def run_headline(args, ws, rank, local):
                                             "traffic_bytes_per_apply:"),
                      "traffic_source": "profiles/toeplitz_apply_warm512.md: DRAM bytes of the "
                                        "three engine kernels of one application (ncu)",
-                     "kernel": "one CG update (A^H A application: k_fwd_plane, k_slow with x Qf, "
-                               "k_inv_plane with the coil sum; FD term; vector updates); bytes "
+                     "kernel": "one CG update (A^H A application: k_fwd_pair, k_slow with x Qf, "
+                               "k_inv_async with the coil sum; FD term; vector updates); bytes "
                                "= the zero-padded FFT model of one A^H A application",
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else
                                     "fallback 6650 GB/s",

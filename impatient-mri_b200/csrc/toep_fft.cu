@@ -684,7 +684,14 @@ constexpr size_t inv_async_smem() {  // k_inv_async: two work planes, twiddle ta
 // per s-parity a, forward FFT along s of x[s] w_2ns^{a s}, x Qf_l (parity a),
 // inverse FFT, times w_2ns^{-a s}; the two parities are summed and written
 // back in place.  Both parities run at once as 2W tile columns (column a W + w
-// holds parity a of spectrum column w): blockDim = 2 W R1, thread (a, w, j1).
+// holds parity a of spectrum column w): blockDim = 2 W R1, and in the stride
+// passes thread (a, j1, w) with a the top bit of the thread index, so that a
+// warp works on one parity.  The parity factor w_2ns^{a (j1 + R1 q)} splits
+// into w_2ns^{a j1}, which commutes with the R2-point DFT and joins the
+// inter-pass twiddle (w_2ns^{j1 (2 k2 + a)}), and w_{2 R2}^{a q}, a
+// compile-time constant.  Tile element (row, col) is stored at
+// row 2W + (col ^ ((row & 1) W)), so that the two rows of a half-warp fall
+// on different bank halves.
 // TWS: the twiddle table sits in shared memory after the tile (else it is read
 // through the read-only global path; the 2-D 512-row instantiation, whose two
 // blocks per SM keep more L1 that way, measures faster so).  STAGE (blocks that
@@ -692,6 +699,19 @@ constexpr size_t inv_async_smem() {  // k_inv_async: two work planes, twiddle ta
 // memory once (cp.async) and read from there by every coil, and the next
 // coil's input columns are copied in while the current coil is transformed.
 constexpr int kSlowThreads = 256;
+
+// w_{2R}^{q} (conjugated when INV), q < R, as compile-time constants.
+template <int R, bool INV>
+struct HalfTw {
+    float c[R], s[R];
+    constexpr HalfTw() : c(), s() {
+        for (int q = 0; q < R; ++q) {
+            const double ang = -3.14159265358979323846264338327950288 * q / R;
+            c[q] = (float)taylor_cos(ang);
+            s[q] = (float)(INV ? -taylor_sin(ang) : taylor_sin(ang));
+        }
+    }
+};
 
 template <int NS, int W>
 struct SlowStage {  // shared-memory layout of the STAGE kernels (float2 offsets)
@@ -724,9 +744,12 @@ __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
     const int col0 = blockIdx.x * W;
     const int lw = WC > 0 ? ilog2c(WC) : __ffs(W) - 1;
     const int W2 = 2 * W, lw2 = lw + 1;
-    const int cw2 = threadIdx.x & (W2 - 1);  // tile column: a W + w
-    const int a = cw2 >> lw, w = cw2 & (W - 1);
-    const int j1 = threadIdx.x >> lw2;
+    const int half = W * R1;                  // threads per parity in the stride passes
+    const int a = threadIdx.x >= half ? 1 : 0;
+    const int rem = threadIdx.x - a * half;
+    const int w = rem & (W - 1), j1 = rem >> lw;
+    const int cw2 = a * W + w;                // tile column
+    auto ei = [&](int row, int col) { return row * W2 + (col ^ ((row & 1) << lw)); };
     const size_t per_coil = (size_t)NS * ncol;
     float2 *Qs = nullptr, *Xs = nullptr;
     if constexpr (STAGE) {
@@ -760,19 +783,24 @@ __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
 #pragma unroll
             for (int q = 0; q < R2; ++q) {
                 const int s = j1 + R1 * q;
-                float2 xv;
-                if constexpr (STAGE) xv = Xs[s * W + w];
-                else xv = bc[(size_t)s * ncol + w];
-                if (a) xv = cmul(xv, wn(tw, s, LNS + 1, false));
-                v[q] = xv;
+                if constexpr (STAGE) v[q] = Xs[s * W + w];
+                else v[q] = bc[(size_t)s * ncol + w];
+            }
+            if (a) {
+                constexpr HalfTw<R2, false> hw{};
+#pragma unroll
+                for (int q = 1; q < R2; ++q) v[q] = cmul(v[q], make_float2(hw.c[q], hw.s[q]));
             }
             dft<R2, false>(v, tw);
-            if (j1 != 0) {
+            if (a) {
+#pragma unroll
+                for (int q = 0; q < R2; ++q) v[q] = cmul(v[q], wn(tw, j1 * (2 * q + 1), LNS + 1, false));
+            } else if (j1 != 0) {
 #pragma unroll
                 for (int q = 1; q < R2; ++q) v[q] = cmul(v[q], wn(tw, j1 * q, LNS, false));
             }
 #pragma unroll
-            for (int q = 0; q < R2; ++q) E[(j1 + R1 * q) * W2 + cw2] = v[q];
+            for (int q = 0; q < R2; ++q) E[ei(j1 + R1 * q, cw2)] = v[q];
         }
         __syncthreads();
         if constexpr (STAGE) {
@@ -784,7 +812,7 @@ __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
             const int aa = cw >> lw, ww = cw & (W - 1);
             float2 z[R1];
 #pragma unroll
-            for (int k1 = 0; k1 < R1; ++k1) z[k1] = E[(k1 + R1 * k2) * W2 + cw];
+            for (int k1 = 0; k1 < R1; ++k1) z[k1] = E[ei(k1 + R1 * k2, cw)];
             dft<R1, false>(z, tw);
 #pragma unroll
             for (int k1 = 0; k1 < R1; ++k1) {
@@ -795,31 +823,33 @@ __global__ void __launch_bounds__(kSlowThreads, 2) k_slow(
                 z[k1] = cmul(z[k1], qv);
             }
             dft<R1, true>(z, tw);
-            if (k2 != 0) {
+            if (k2 != 0 || aa) {  // w_2ns^{-j (2 k2 + aa)}: with the parity's j1 factor
 #pragma unroll
-                for (int j = 1; j < R1; ++j) z[j] = cmul(z[j], wn(tw, j * k2, LNS, true));
+                for (int j = 1; j < R1; ++j)
+                    z[j] = cmul(z[j], wn(tw, j * (2 * k2 + aa), LNS + 1, true));
             }
 #pragma unroll
-            for (int j = 0; j < R1; ++j) E[(j + R1 * k2) * W2 + cw] = z[j];
+            for (int j = 0; j < R1; ++j) E[ei(j + R1 * k2, cw)] = z[j];
         }
         __syncthreads();
-        {   // stride pass, inverse, parity twiddle
+        {   // stride pass, inverse, the constant part of the parity twiddle
             float2 v[R2];
 #pragma unroll
-            for (int q = 0; q < R2; ++q) v[q] = E[(j1 + R1 * q) * W2 + cw2];
+            for (int q = 0; q < R2; ++q) v[q] = E[ei(j1 + R1 * q, cw2)];
             dft<R2, true>(v, tw);
+            if (a) {
+                constexpr HalfTw<R2, true> hw{};
 #pragma unroll
-            for (int q = 0; q < R2; ++q) {
-                float2 xv = v[q];
-                if (a) xv = cmul(xv, wn(tw, j1 + R1 * q, LNS + 1, true));
-                E[(j1 + R1 * q) * W2 + cw2] = xv;
+                for (int q = 1; q < R2; ++q) v[q] = cmul(v[q], make_float2(hw.c[q], hw.s[q]));
             }
+#pragma unroll
+            for (int q = 0; q < R2; ++q) E[ei(j1 + R1 * q, cw2)] = v[q];
         }
         __syncthreads();
         // parity sum, written back in place (W consecutive columns per row)
         for (int it = threadIdx.x; it < NS * W; it += blockDim.x) {
             const int sidx = it >> lw, ww = it & (W - 1);
-            bc[(size_t)sidx * ncol + ww] = cadd(E[sidx * W2 + ww], E[sidx * W2 + W + ww]);
+            bc[(size_t)sidx * ncol + ww] = cadd(E[ei(sidx, ww)], E[ei(sidx, W + ww)]);
         }
     }
 }

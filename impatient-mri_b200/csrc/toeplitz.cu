@@ -168,20 +168,33 @@ __global__ void __launch_bounds__(kGridWarps * 32)
                                : kb_weight(fabsf(cc[a] - (float)(lo[a] + j)) * inv_os, g.beta);
         }
         __syncwarp();
+        // Shifted index lo + j + gs / 2 of a covered cell is below 2 gs: it wraps
+        // at most once (one conditional subtraction, no division per cell).  The
+        // loop axis steps by a fixed stride and wraps once.
         const int nbc = cnt[B] * cnt[Cc];
+        int a0 = g.is3d ? lo[A] + g.gs[A] / 2 : 0;
+        if (a0 >= g.gs[A]) a0 -= g.gs[A];
+        const size_t astride = g.is3d ? (size_t)g.gs[1] * g.gs[2] : 0;
+        const size_t awrap = astride * g.gs[A];
+        const int rowlen = g.is3d ? g.gs[2] : g.gs[1];  // stride of axis B
         for (int p = lane; p < nbc; p += 32) {
             const int jb = p / cnt[Cc], jc = p - jb * cnt[Cc];
             const float wbc = ws[B][jb] * ws[Cc][jc];
             if (wbc == 0.f) continue;
-            int idx[3];
-            idx[B] = (lo[B] + jb + g.gs[B] / 2) % g.gs[B];
-            idx[Cc] = (lo[Cc] + jc + g.gs[Cc] / 2) % g.gs[Cc];
+            int ib = lo[B] + jb + g.gs[B] / 2;
+            if (ib >= g.gs[B]) ib -= g.gs[B];
+            int ic = lo[Cc] + jc + g.gs[Cc] / 2;
+            if (ic >= g.gs[Cc]) ic -= g.gs[Cc];
+            size_t cell = (size_t)a0 * astride + (size_t)ib * rowlen + ic;
+            int ia = a0;
             for (int ja = 0; ja < cnt[A]; ++ja) {
                 const float ww = wbc * ws[A][ja];
-                if (ww == 0.f) continue;
-                idx[A] = g.is3d ? (lo[A] + ja + g.gs[A] / 2) % g.gs[A] : 0;
-                const size_t cell = ((size_t)idx[0] * g.gs[1] + idx[1]) * g.gs[2] + idx[2];
-                atomicAdd(&grid[cell], make_float2(ww * vr, ww * vi));
+                if (ww != 0.f) atomicAdd(&grid[cell], make_float2(ww * vr, ww * vi));
+                cell += astride;
+                if (++ia == g.gs[A]) {
+                    ia = 0;
+                    cell -= awrap;
+                }
             }
         }
         __syncwarp();  // the next sample overwrites ws
