@@ -110,6 +110,8 @@ public:
 private:
     cudaError_t run_init();
     cudaError_t run_iteration();
+    cudaError_t set_table(bool adj, int split);
+    cudaError_t tune_shapes(bool adj);
 
     BfConfig cfg_;
     NuPlan plan_;          // C, CG, G, Npad, use_z and the shared sensitivities

@@ -380,7 +380,8 @@ cudaError_t BfBatch::setup(const BfConfig &cfg, int S, const int *k_off, const f
     plan_.kgeo = kgeo_;
     plan_.vgeo = vgeo_;
     plan_.sens = sens_;
-    // one launch shape for every slice
+    // one launch shape for every slice: the heuristic, replaced by the batch's
+    // tuned shape (tune_shapes) when tuning is on
     fwd_ = nu_default_launch(plan_, false);
     adj_ = nu_default_launch(plan_, true);
     const int fwd_rows = fwd_.tc ? nu_tc_rows(CG) : kNT * fwd_.pt;
@@ -388,22 +389,11 @@ cudaError_t BfBatch::setup(const BfConfig &cfg, int S, const int *k_off, const f
     fwd_.split = batch_split((long long)(mpad_total_ / fwd_rows) * G, std::vector<int>{Npad},
                              fwd_.tc != 0);
     adj_.split = batch_split((long long)(Npad / adj_rows) * G * S, mpad_, adj_.tc != 0);
-    std::vector<NuSlice> tf(S), ta(S);
     std::vector<BbSlice> tv(S);
-    for (int s = 0; s < S; ++s) {
-        const long long ko = koff_pad_[s];
-        tf[s] = NuSlice{ko, (long long)s * Npad, (long long)s * G * Npad * CG,
-                        (long long)fwd_.split * G * CG * ko, mpad_[s], Npad, Npad / fwd_.split};
-        ta[s] = NuSlice{(long long)s * Npad, ko, (long long)G * CG * ko,
-                        (long long)s * adj_.split * G * Npad, Npad, mpad_[s],
-                        mpad_[s] / adj_.split};
-        tv[s] = BbSlice{ko, m_[s], mpad_[s], (long long)k_off[s]};
-    }
+    for (int s = 0; s < S; ++s) tv[s] = BbSlice{koff_pad_[s], m_[s], mpad_[s], (long long)k_off[s]};
     BB_TRY(dalloc(&tab_fwd_, S));
     BB_TRY(dalloc(&tab_adj_, S));
     BB_TRY(cudaMalloc(&tab_vec_, sizeof(BbSlice) * S));
-    BB_TRY(cudaMemcpyAsync(tab_fwd_, tf.data(), sizeof(NuSlice) * S, cudaMemcpyHostToDevice, st));
-    BB_TRY(cudaMemcpyAsync(tab_adj_, ta.data(), sizeof(NuSlice) * S, cudaMemcpyHostToDevice, st));
     BB_TRY(cudaMemcpyAsync(tab_vec_, tv.data(), sizeof(BbSlice) * S, cudaMemcpyHostToDevice, st));
     const size_t nk = (size_t)mpad_total_ * G * CG;
     BB_TRY(dalloc(&y_, nk));
@@ -415,13 +405,131 @@ cudaError_t BfBatch::setup(const BfConfig &cfg, int S, const int *k_off, const f
     BB_TRY(dalloc(&g_, (size_t)S * Npad));
     BB_TRY(dalloc(&d_, (size_t)S * Npad));
     BB_TRY(dalloc(&w_, (size_t)S * Npad));
+    BB_TRY(tune_shapes(false));
+    BB_TRY(tune_shapes(true));
+    BB_TRY(set_table(false, fwd_.split));
+    BB_TRY(set_table(true, adj_.split));
     BB_TRY(dalloc(&pf_, nk * fwd_.split));
     BB_TRY(dalloc(&pa_, (size_t)S * adj_.split * G * Npad));
     kb_ = std::max(2, std::min(kDotBlocks, (kDotBlocks + S - 1) / S));
     BB_TRY(dalloc(&dots_, (size_t)S * 5 * kb_));
     BB_TRY(cudaMemsetAsync(dots_, 0, sizeof(double) * S * 5 * kb_, st));
-    // the slice tables are copied from host vectors that end with this call
     return cudaStreamSynchronize(st);
+}
+
+// Per-slice table of one direction for a given split (see NuSlice).
+cudaError_t BfBatch::set_table(bool adj, int split) {
+    const int S = S_, G = plan_.G, CG = plan_.CG, Npad = plan_.Npad;
+    std::vector<NuSlice> tab(S);
+    for (int s = 0; s < S; ++s) {
+        const long long ko = koff_pad_[s];
+        tab[s] = adj ? NuSlice{(long long)s * Npad, ko, (long long)G * CG * ko,
+                               (long long)s * split * G * Npad, Npad, mpad_[s], mpad_[s] / split}
+                     : NuSlice{ko, (long long)s * Npad, (long long)s * G * Npad * CG,
+                               (long long)split * G * CG * ko, mpad_[s], Npad, Npad / split};
+    }
+    BB_TRY(cudaMemcpyAsync(adj ? tab_adj_ : tab_fwd_, tab.data(), sizeof(NuSlice) * S,
+                           cudaMemcpyHostToDevice, st_));
+    return cudaStreamSynchronize(st_);  // `tab` ends with this call
+}
+
+// Launch shape of one direction for the whole batch: a cached result for this
+// batched problem, else (tuning on) every candidate -- within the heuristic's
+// kernel family, splits from half to four times the heuristic's that cut every
+// slice into whole tiles and keep the partial sums within twice the
+// heuristic's (at least 1 GB); for the CUDA-core kernel also every supported
+// pt and both register budgets -- timed once over the whole batch with CUDA
+// events on the batch's stream (inputs zeroed; the timing does not depend on
+// the values), the fastest kept and cached.
+cudaError_t BfBatch::tune_shapes(bool adj) {
+    NuLaunch &l = adj ? adj_ : fwd_;
+    const int G = plan_.G, CG = plan_.CG, Npad = plan_.Npad;
+    const NuBatchKey key{adj ? 1 : 0, CG, G, plan_.use_z ? 1 : 0, S_, Npad, max_mpad_,
+                         mpad_total_, l.tc};
+    NuLaunch cached;
+    if (nu_batch_lookup(key, &cached)) {
+        l = cached;
+        return cudaSuccess;
+    }
+    if (!nu_tuning_enabled()) return cudaSuccess;
+    const std::vector<int> ranges = adj ? mpad_ : std::vector<int>{Npad};
+    auto split_ok = [&](int sp) {
+        for (int r : ranges)
+            if (!nu_split_ok(r, sp) || r / sp < 2 * kTile) return false;
+        return true;
+    };
+    const size_t per_split = adj ? (size_t)S_ * G * Npad : (size_t)mpad_total_ * G * CG;
+    const size_t cap = std::max(2 * per_split * l.split, (size_t(1) << 30) / sizeof(float2));
+    std::vector<NuLaunch> cands;
+    std::vector<int> pts, occs;
+    if (l.tc) {
+        pts = {l.pt};
+        occs = {l.occ};
+    } else {
+        for (int pt : {2, 4, 8})
+            if (nu_shape_supported(CG, pt)) pts.push_back(pt);
+        occs = {4, 6};
+    }
+    int max_split = 0;
+    for (int pt : pts)
+        for (int occ : occs)
+            for (int sp = std::max(1, l.split / 2); sp <= std::min(64, 4 * l.split); sp *= 2) {
+                if (!split_ok(sp) || per_split * sp > cap) continue;
+                NuLaunch c = l;
+                c.pt = pt;
+                c.occ = occ;
+                c.split = sp;
+                cands.push_back(c);
+                max_split = std::max(max_split, sp);
+            }
+    if (cands.size() < 2) {
+        nu_batch_store(key, l, 0.0);
+        return cudaSuccess;
+    }
+    float2 *part = nullptr;
+    BB_TRY(dalloc(&part, per_split * max_split));
+    const float2 *in = adj ? rpk_ : xs_;
+    const size_t in_elems = adj ? (size_t)mpad_total_ * G * CG : (size_t)S_ * G * Npad * CG;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaMemsetAsync(const_cast<float2 *>(in), 0, sizeof(float2) * in_elems, st_);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    const int max_ours = adj ? Npad : max_mpad_;
+    auto run = [&](const NuLaunch &c) {
+        return adj ? nu_partials_batch(plan_, c, true, S_, max_ours, tab_adj_, vgeo_, kgeo_, in,
+                                       part, err_, st_)
+                   : nu_partials_batch(plan_, c, false, S_, max_ours, tab_fwd_, kgeo_, vgeo_, in,
+                                       part, err_, st_);
+    };
+    float best = 1e30f;
+    NuLaunch best_l = l;
+    int table_split = -1;
+    for (size_t i = 0; i < cands.size() && e == cudaSuccess; ++i) {
+        const NuLaunch &c = cands[i];
+        if (c.split != table_split) {
+            e = set_table(adj, c.split);
+            table_split = c.split;
+            if (e != cudaSuccess) break;
+        }
+        if (i == 0 && (e = run(c)) != cudaSuccess) break;  // first use: module and caches warm
+        cudaEventRecord(e0, st_);
+        if ((e = run(c)) != cudaSuccess) break;
+        cudaEventRecord(e1, st_);
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+            best = ms;
+            best_l = c;
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(part);
+    if (e != cudaSuccess) return e;
+    l = best_l;
+    nu_batch_store(key, l, best);
+    return cudaSuccess;
 }
 
 cudaError_t BfBatch::run_init() {

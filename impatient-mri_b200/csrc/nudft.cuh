@@ -149,4 +149,18 @@ bool nu_tuned_lookup(const NuPlan &p, bool adj, NuLaunch *out);
 // Largest partial-sum scratch any tuning candidate needs.
 size_t nu_tune_partial_bytes(const NuPlan &p, bool adj);
 
+// Batched launches (one shape for all slices): the launch shape within the
+// kernel family of the plan (tensor-core: split; CUDA-core: pt, occupancy and
+// split) is tuned per batched problem -- direction, coil grouping, slice count
+// and padded sizes -- by timing the whole batch, and cached beside the
+// single-slice shapes (lines "b1 ...").
+struct NuBatchKey {
+    int adj, CG, G, use_z, S, Npad, max_mpad;
+    long long mpad_total;
+    int tc;
+};
+bool nu_tuning_enabled();
+bool nu_batch_lookup(const NuBatchKey &k, NuLaunch *out);
+void nu_batch_store(const NuBatchKey &k, const NuLaunch &l, double ms);
+
 }  // namespace imp

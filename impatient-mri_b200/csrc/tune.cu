@@ -7,6 +7,8 @@
 // the launching stream, and keeps the fastest.
 // Results are cached per shape in memory and persisted as text lines
 //     v2 <adj> <CG> <G> <use_z> <Mpad> <Npad> <pt> <occ> <split> <tc> <ms>
+// and, for batched launches (the split only, timed by the batch itself),
+//     b1 <adj> <CG> <G> <use_z> <S> <Npad> <max Mpad> <sum Mpad> <tc> <pt> <occ> <split> <ms>
 // in $IMP_TUNE_CACHE (default ~/.cache/impatient_b200/nudft_tune.txt), so a
 // shape is tuned once per machine.  IMP_AUTOTUNE=0 turns tuning and the use of
 // tuned shapes off (default launch shapes only).
@@ -29,7 +31,13 @@ using Key = std::tuple<int, int, int, int, int, int>;
 
 std::mutex g_mu;
 std::map<Key, NuLaunch> g_cache;
+using BKey = std::tuple<int, int, int, int, int, int, int, long long, int>;
+std::map<BKey, NuLaunch> g_bcache;  // batched problems
 bool g_loaded = false;
+
+BKey bkey_of(const NuBatchKey &k) {
+    return BKey(k.adj, k.CG, k.G, k.use_z, k.S, k.Npad, k.max_mpad, k.mpad_total, k.tc);
+}
 
 Key key_of(const NuPlan &p, bool adj) {
     return Key(adj ? 1 : 0, p.CG, p.G, p.use_z ? 1 : 0, p.Mpad, p.Npad);
@@ -50,6 +58,20 @@ void load_locked() {
     while (std::fgets(line, sizeof line, f)) {
         int a, cg, g, z, mp, np, pt, occ, split, tc;
         double ms;
+        NuBatchKey b;
+        if (std::sscanf(line, "b1 %d %d %d %d %d %d %d %lld %d %d %d %d %lf", &b.adj, &b.CG, &b.G,
+                        &b.use_z, &b.S, &b.Npad, &b.max_mpad, &b.mpad_total, &b.tc, &pt, &occ,
+                        &split, &ms) == 13) {
+            NuLaunch l;
+            l.tc = b.tc;
+            l.pt = pt;
+            l.occ = occ;
+            l.split = split;
+            const bool ok = b.tc ? nu_tc_supported(b.CG)
+                                 : (nu_shape_supported(b.CG, pt) && (occ == 4 || occ == 6));
+            if (ok && split >= 1 && split <= 64) g_bcache[bkey_of(b)] = l;
+            continue;
+        }
         if (std::sscanf(line, "v2 %d %d %d %d %d %d %d %d %d %d %lf", &a, &cg, &g, &z, &mp, &np,
                         &pt, &occ, &split, &tc, &ms) != 11)
             continue;  // other versions are re-tuned
@@ -83,6 +105,16 @@ bool tuning_enabled() {
     return !(e && e[0] == '0');
 }
 
+void append_line(const char *text) {
+    std::string path = cache_path();
+    for (size_t i = 1; i < path.size(); ++i)
+        if (path[i] == '/') mkdir(path.substr(0, i).c_str(), 0755);
+    FILE *f = std::fopen(path.c_str(), "a");
+    if (!f) return;  // the cache is an optimisation; failure to write is not an error
+    std::fputs(text, f);
+    std::fclose(f);
+}
+
 std::vector<int> pts_for(int CG) {
     std::vector<int> v;
     for (int pt : {2, 4, 8})
@@ -94,6 +126,29 @@ constexpr int kMaxSplit = 64;
 constexpr size_t kMaxPartialBytes = size_t(512) << 20;
 
 }  // namespace
+
+bool nu_tuning_enabled() { return tuning_enabled(); }
+
+bool nu_batch_lookup(const NuBatchKey &k, NuLaunch *out) {
+    if (!tuning_enabled()) return false;
+    std::lock_guard<std::mutex> g(g_mu);
+    load_locked();
+    auto it = g_bcache.find(bkey_of(k));
+    if (it == g_bcache.end()) return false;
+    *out = it->second;
+    return true;
+}
+
+void nu_batch_store(const NuBatchKey &k, const NuLaunch &l, double ms) {
+    std::lock_guard<std::mutex> g(g_mu);
+    load_locked();
+    g_bcache[bkey_of(k)] = l;
+    char line[256];
+    std::snprintf(line, sizeof line, "b1 %d %d %d %d %d %d %d %lld %d %d %d %d %.4f\n", k.adj,
+                  k.CG, k.G, k.use_z, k.S, k.Npad, k.max_mpad, k.mpad_total, k.tc, l.pt, l.occ,
+                  l.split, ms);
+    append_line(line);
+}
 
 size_t nu_tune_partial_bytes(const NuPlan &p, bool adj) {
     const int n_theirs = adj ? p.Mpad : p.Npad;
