@@ -61,7 +61,7 @@ struct TScal {
     int done;
     double tol;   // stop when sqrt(|r|^2 / |F^H d|^2) < tol
     int iters;    // CG updates performed since the solve started
-    int pad;
+    unsigned arrive;  // k_t_dir blocks done with this update (the last one finishes it)
 };
 
 __device__ __forceinline__ TScal *scal(double *dots) {
@@ -384,12 +384,15 @@ __global__ void k_crop_acc(float2 *acc, const float2 *big, const float2 *sens,
 
 // q += lambda D^H W D p (pen 1) or lambda C^T W C p (pen 2, y = W C p formed
 // beforehand); partial Re<p, q>
-__global__ void __launch_bounds__(kVB) k_t_tvdot(float2 *q, const float2 *p, const float *w,
-                                                 int N, Grid3 gd, int pen, float lambda,
-                                                 RegView reg, double *dots) {
+__global__ void __launch_bounds__(kVB) k_t_tvdot(float2 *__restrict__ q,
+                                                 const float2 *__restrict__ p,
+                                                 const float *__restrict__ w, int N, Grid3 gd,
+                                                 int pen, float lambda, RegView reg,
+                                                 double *dots) {
     __shared__ double sh[33];
     if (scal(dots)->done) return;
     double loc = 0.0;
+#pragma unroll 4
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < N; r += gridDim.x * blockDim.x) {
         float2 v = q[r];
         if (pen) {
@@ -406,14 +409,17 @@ __global__ void __launch_bounds__(kVB) k_t_tvdot(float2 *q, const float2 *p, con
 }
 
 // alpha = beta2 / Re<p,q>; x += alpha p; r -= alpha q; partial |r|^2
-__global__ void __launch_bounds__(kVB) k_t_update(float2 *x, float2 *r, const float2 *p,
-                                                  const float2 *q, int N, double *dots) {
+__global__ void __launch_bounds__(kVB) k_t_update(float2 *__restrict__ x, float2 *__restrict__ r,
+                                                  const float2 *__restrict__ p,
+                                                  const float2 *__restrict__ q, int N,
+                                                  double *dots) {
     __shared__ double sh[33];
     TScal *S = scal(dots);
     if (S->done) return;
     const double pq = sum_partials(dots + T_PQ * kTBlocks, kTBlocks, sh);
     const float alpha = (float)(S->beta2[S->cur] / pq);
     double loc = 0.0;
+#pragma unroll 4
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const float2 pv = p[i], qv = q[i];
         float2 xv = x[i], rv = r[i];
@@ -429,38 +435,49 @@ __global__ void __launch_bounds__(kVB) k_t_update(float2 *x, float2 *r, const fl
     if (threadIdx.x == 0) dots[T_RR * kTBlocks + blockIdx.x] = b;
 }
 
-// p = r + (beta2_new / beta2) p; best-residual tracking
-__global__ void __launch_bounds__(kVB) k_t_dir(float2 *p, const float2 *r, const float2 *x,
-                                               float2 *best, int N, double *dots) {
+// p = r + (beta2_new / beta2) p; best-residual tracking.  The last block to
+// finish (arrival counter) closes the update: best residual, beta2 swap,
+// iteration count and the stopping test (recon.cu:2107-2112).  Every block
+// has read the scalars it uses before it arrives, so the update of the
+// scalars cannot race with those reads.
+__global__ void __launch_bounds__(kVB) k_t_dir(float2 *__restrict__ p,
+                                               const float2 *__restrict__ r,
+                                               const float2 *__restrict__ x,
+                                               float2 *__restrict__ best, int N, double *dots) {
     __shared__ double sh[33];
     TScal *S = scal(dots);
     if (S->done) return;
     const double bnew = sum_partials(dots + T_RR * kTBlocks, kTBlocks, sh);
-    const double bold = S->beta2[S->cur];
+    const int cur = S->cur;
+    const double bold = S->beta2[cur];
     const float ratio = (float)(bnew / bold);
     const bool better = bnew < S->res_best;
+#pragma unroll 4
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         const float2 rv = r[i], pv = p[i];
         p[i] = make_float2(rv.x + ratio * pv.x, rv.y + ratio * pv.y);
         if (better) best[i] = x[i];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) S->beta2[S->cur ^ 1] = bnew;
-}
-
-__global__ void k_t_finish(double *dots) {
-    TScal *S = scal(dots);
-    if (S->done) return;
-    const double bnew = S->beta2[S->cur ^ 1];
-    if (bnew < S->res_best) S->res_best = bnew;
-    S->cur ^= 1;
-    S->iters += 1;
-    if (sqrt(bnew / S->norm_fhd) < S->tol) S->done = 1;
+    __syncthreads();  // the block's reads of the scalars are done
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&S->arrive, 1u) == gridDim.x - 1) {
+            __threadfence();
+            S->beta2[cur ^ 1] = bnew;
+            if (bnew < S->res_best) S->res_best = bnew;
+            S->cur = cur ^ 1;
+            S->iters += 1;
+            if (sqrt(bnew / S->norm_fhd) < S->tol) S->done = 1;
+            S->arrive = 0;
+        }
+    }
 }
 
 __global__ void k_t_setup(double *dots, double tol) {
     TScal *S = scal(dots);
     S->tol = tol;
     S->iters = 0;
+    S->arrive = 0;
 }
 
 // TV-pass start: r = fhd - q; p = r; partial |r|^2
@@ -866,7 +883,6 @@ cudaError_t ToepSolver::cg_iteration() {
     T_TRY(penalty_dot(q_, p_));
     k_t_update<<<kTBlocks, kVB, 0, st_>>>(x_, r_, p_, q_, (int)N_, dots_);
     k_t_dir<<<kTBlocks, kVB, 0, st_>>>(p_, r_, x_, best_, (int)N_, dots_);
-    k_t_finish<<<1, 1, 0, st_>>>(dots_);
     return cudaGetLastError();
 }
 
@@ -901,7 +917,7 @@ cudaError_t ToepSolver::solve(const float *fhd_r, const float *fhd_i, float *x_r
     k_t_setup<<<1, 1, 0, st_>>>(dots_, 1.0e-16);  // recon.cu:2112
     T_TRY(cudaGetLastError());
     launches_ += 5;
-    const int iter_launches = 3 * (L_ + 1) + 4;  // own kernels of one CG iteration
+    const int iter_launches = 3 * (L_ + 1) + 3 + (reg_.on() ? 1 : 0);  // one CG iteration
     if (cfg_.use_graphs && !g_iter_) T_TRY(capture_graph(st_, &g_iter_, &ToepSolver::cg_iteration, this));
     for (int tv_i = 0; tv_i < std::max(cfg_.tv ? cfg_.tv_num : 1, 1); ++tv_i) {
         if (tv_i != 0) {
@@ -959,7 +975,7 @@ cudaError_t ToepSolver::solve_from(const float *fhd_r, const float *fhd_i, float
     k_t_init_finish<<<1, kVB, 0, st_>>>(dots_);
     T_TRY(cudaGetLastError());
     launches_ += 3 * (L_ + 1) + 3;
-    const int iter_launches = 3 * (L_ + 1) + 4;
+    const int iter_launches = 3 * (L_ + 1) + 3 + (reg_.on() ? 1 : 0);
     const TScal *S = reinterpret_cast<const TScal *>(dots_ + T_SCAL * kTBlocks);
     int it = 0;
     while (it < max_iter) {
