@@ -218,6 +218,32 @@ def test_apply_production_sizes_match_oracle(pkg, ctx, dims):
 
 
 @pytest.mark.parametrize("dims", [(256, 256, 32), (512, 512, 1)])
+def test_apply_many_coils_per_block_match_oracle(pkg, ctx, dims):
+    """Sixteen coils at the benchmark sizes: the inverse plane kernel's cluster of
+    8 blocks gives each block two coils (register partial sums over both, the
+    next quadrant's copies across the coil boundary), and in 3-D each slow-axis
+    block loops over all 16 coils with the next coil's columns copied in ahead;
+    one application against the FP64 oracle (2 segments)."""
+    rng = np.random.default_rng(sum(dims) + 303)
+    nx, ny, nz = dims
+    C, L, M = 16, 1, 64
+    N, G = nx * ny * nz, grid_elems(dims)
+    c = dict(dims=dims, L=L, cg=1, fdp=1e-2, tv_num=0, os_q=2.0, os_fh=1.5,
+             t=np.sort(rng.uniform(0.0, 0.01, M)).astype(np.float32),
+             kx=np.zeros(M, np.float32),
+             fm=rng.uniform(-300.0, 300.0, N).astype(np.float32),
+             sens=(rng.standard_normal((C, N)) + 1j * rng.standard_normal((C, N))).astype(
+                 np.complex64))
+    Q = (rng.standard_normal((L + 1, G)) + 1j * rng.standard_normal((L + 1, G))).astype(
+        np.complex64)
+    p = (rng.standard_normal(N) + 1j * rng.standard_normal(N)).astype(np.complex64)
+    got = gpu_apply(pkg, ctx, opts_of(pkg, c), c, Q, p)
+    err = rel(got, oracle_apply(c, Q, p, c["fdp"]))
+    print(f"apply {dims} C={C} L={L}: {err:.2e} vs the FP64 oracle")
+    assert err < TOL_OP
+
+
+@pytest.mark.parametrize("dims", [(256, 256, 32), (512, 512, 1)])
 def test_specialised_plane_kernels_match_generic(pkg, monkeypatch, dims):
     """The plane kernels instantiated on compile-time geometry (3-D 256x256x32
     and 2-D 512x512 images) give the A^H A application of the generic
