@@ -570,7 +570,10 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_plane(
 // staging buffer and no scatter pass.  Each thread keeps the partial coil sum
 // of its own elements in registers; after the last quadrant the sums go to
 // shared memory (over the work planes) for the cluster's coil reduction.
-template <class Geo>
+// ONE_COIL (every block has exactly one coil: C <= cluster size): the quadrants
+// are summed first and conj(S_c) applied once at the end, one sensitivity read
+// per element instead of one per quadrant.
+template <class Geo, bool ONE_COIL = false>
 __global__ void __launch_bounds__(kPlaneThreads) k_inv_async(
     float2 *__restrict__ q, const float2 *__restrict__ b1, const float2 *__restrict__ sens,
     const float2 *__restrict__ eph_l, Geo g, int first, const float2 *__restrict__ tw_g,
@@ -652,7 +655,16 @@ __global__ void __launch_bounds__(kPlaneThreads) k_inv_async(
                 float2 val = P[pp * pstride + m * Geo::rs + fphys(g, fth)];
                 if (am) val = cmul(val, wn(tw, m, Geo::lnm + 1, true));
                 if (af) val = cmul(val, wf);
-                y[i] = cadd(y[i], cmulc(__ldg(&sc[e]), val));
+                if constexpr (ONE_COIL) y[i] = cadd(y[i], val);
+                else y[i] = cadd(y[i], cmulc(__ldg(&sc[e]), val));
+            }
+        }
+        if constexpr (ONE_COIL) {
+            if (nq > 0) {
+                const float2 *sc = sens + (size_t)rank * N + vbase;
+#pragma unroll
+                for (int i = 0; i < VPT; ++i)
+                    y[i] = cmulc(__ldg(&sc[threadIdx.x + i * kPlaneThreads]), y[i]);
             }
         }
         __syncthreads();  // the work planes become the partial-sum array
@@ -899,9 +911,15 @@ cudaError_t set_plane_smem(size_t fwd_bytes, size_t inv_bytes) {
     if constexpr (std::is_same<Geo, PlaneGeo>::value)
         return cudaFuncSetAttribute(k_inv_plane<VPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)inv_bytes);
-    else
-        return cudaFuncSetAttribute(k_inv_async<Geo>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    else {
+        cudaError_t e2 = cudaFuncSetAttribute(k_inv_async<Geo>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)inv_async_smem<Geo>());
+        if (e2 != cudaSuccess) return e2;
+        return cudaFuncSetAttribute(k_inv_async<Geo, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)inv_async_smem<Geo>());
+    }
 }
 
 // Plane geometries with compile-time instantiations: 3-D 256 x 256 x 32 images
@@ -1143,9 +1161,16 @@ cudaError_t toep_fft_apply_l(const ToepFftPlan &p, float2 *q, const float2 *x,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     cudaError_t e;
-    if (spec == 1)
+    const bool one_coil = p.C == p.csize;  // cluster rank r takes coil r only
+    if (spec == 1 && one_coil)
+        e = cudaLaunchKernelEx(&cfg, k_inv_async<GeoC3d, true>, q, b1, sens, eph_l,
+                               geo_c<GeoC3d>(p), first, tw, done);
+    else if (spec == 1)
         e = cudaLaunchKernelEx(&cfg, k_inv_async<GeoC3d>, q, b1, sens, eph_l, geo_c<GeoC3d>(p),
                                first, tw, done);
+    else if (spec == 2 && one_coil)
+        e = cudaLaunchKernelEx(&cfg, k_inv_async<GeoC2d, true>, q, b1, sens, eph_l,
+                               geo_c<GeoC2d>(p), first, tw, done);
     else if (spec == 2)
         e = cudaLaunchKernelEx(&cfg, k_inv_async<GeoC2d>, q, b1, sens, eph_l, geo_c<GeoC2d>(p),
                                first, tw, done);
